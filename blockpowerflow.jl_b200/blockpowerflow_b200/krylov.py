@@ -1,0 +1,125 @@
+"""block_gmres / block_bicgstab with the reference's keyword arguments and stats types.
+
+Mirrors src/block_gmres.jl:127-154 and src/block_bicgstab.jl:182-185: same argument
+meaning, same defaults, same status strings, same error cases; the work runs in libbpf.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import math
+
+import numpy as np
+
+from . import _lib
+from .sparse import CuSparseMatrixCSR, colmajor, empty_colmajor, ld
+
+_SQRT_EPS = math.sqrt(np.finfo(np.float64).eps)
+
+
+@dataclasses.dataclass
+class BlockGMRESStats:
+    """BlockGMRESStats (src/block_utils.jl:62-68)."""
+    niter: int
+    solved: bool
+    residuals: list
+    timer: float
+    status: str
+    npass: int = 0
+
+
+@dataclasses.dataclass
+class SimpleStats:
+    """SimpleStats (src/block_bicgstab.jl:15-21)."""
+    niter: int
+    solved: bool
+    residuals: list
+    timer: float
+    status: str
+
+
+def _status_string(code: int) -> str:
+    return _lib.load().bpf_solve_status_string(code).decode()
+
+
+def _prec_handle(P):
+    if P is None:
+        return None
+    return P.handle
+
+
+def block_gmres(A: CuSparseMatrixCSR, B, X0=None, *, memory: int = 20, M=None, N=None,
+                ldiv: bool = False, restart: bool = False, reorthogonalization: bool = False,
+                atol: float = _SQRT_EPS, rtol: float = _SQRT_EPS, itmax: int = 0,
+                timemax: float = math.inf, verbose: int = 0, history: bool = False):
+    """(X, stats) = block_gmres(A, B[, X0]; kwargs...)  (src/block_gmres.jl:127-154).
+
+    M / N: left / right preconditioner (None = identity), applied with ldiv! when ldiv=True.
+    """
+    Bc = colmajor(B)
+    n, p = Bc.shape
+    if A.n != n:
+        raise _lib.DimensionMismatch(_lib.BPF_ERR_DIMENSION, "Inconsistent problem size")
+    X = empty_colmajor(n, p, Bc.device)
+    x0p, ldx0 = None, n
+    if X0 is not None:
+        X0c = colmajor(X0)
+        if tuple(X0c.shape) != (n, p):
+            raise _lib.DimensionMismatch(_lib.BPF_ERR_DIMENSION, f"X0 should have size ({n}, {p})")
+        x0p, ldx0 = X0c.data_ptr(), ld(X0c)
+    lib = _lib.load()
+    ctx = _lib.context(Bc.device.index)
+    opts = _lib.GmresOpts(int(memory), int(bool(restart)), int(bool(reorthogonalization)),
+                          int(bool(ldiv)), float(atol), float(rtol), int(itmax),
+                          float(timemax) if math.isfinite(timemax) else 0.0, int(verbose),
+                          int(bool(history)))
+    cap = (int(itmax) if itmax else 2 * (n // max(p, 1))) + 2
+    res = np.zeros(max(cap, 1))
+    st = _lib.Stats(0, 0, 0, 0.0, 0, len(res), res.ctypes.data_as(C.POINTER(C.c_double)), 0)
+    d = A.desc()
+    _lib.check(lib.bpf_block_gmres(ctx, C.byref(d), p, Bc.data_ptr(), ld(Bc), X.data_ptr(), ld(X),
+                                   x0p, ldx0, _prec_handle(M), _prec_handle(N), C.byref(opts),
+                                   C.byref(st)), ctx)
+    stats = BlockGMRESStats(st.niter, bool(st.solved),
+                            res[: min(st.n_residuals, len(res))].tolist() if history else [],
+                            st.timer, _status_string(st.status), st.npass)
+    return X, stats
+
+
+def block_bicgstab(A: CuSparseMatrixCSR, B, *, C=None, N=None, atol: float = _SQRT_EPS,
+                   rtol: float = _SQRT_EPS, itmax: int = 0, timemax: float = math.inf,
+                   verbose: int = 0, history: bool = False):
+    """(X, stats) = block_bicgstab(A, B; C=B, N, kwargs...)  (src/block_bicgstab.jl:182-299).
+
+    N (None = identity) is applied as Y = N \\ P, the operation the reference's comment at
+    src/block_bicgstab.jl:247 describes.
+    """
+    import ctypes
+
+    Bc = colmajor(B)
+    n, p = Bc.shape
+    if A.n != n:
+        raise _lib.DimensionMismatch(_lib.BPF_ERR_DIMENSION, "Inconsistent problem size")
+    X = empty_colmajor(n, p, Bc.device)
+    cp, ldc = None, n
+    if C is not None:
+        Cc = colmajor(C)
+        if tuple(Cc.shape) != (n, p):
+            raise _lib.DimensionMismatch(_lib.BPF_ERR_DIMENSION, "C should have the size of B")
+        cp, ldc = Cc.data_ptr(), ld(Cc)
+    lib = _lib.load()
+    ctx = _lib.context(Bc.device.index)
+    opts = _lib.BicgstabOpts(float(atol), float(rtol), int(itmax),
+                             float(timemax) if math.isfinite(timemax) else 0.0, int(verbose),
+                             int(bool(history)))
+    cap = (int(itmax) if itmax else 2 * n) + 2
+    res = np.zeros(max(cap, 1))
+    st = _lib.Stats(0, 0, 0, 0.0, 0, len(res), res.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 0)
+    d = A.desc()
+    _lib.check(lib.bpf_block_bicgstab(ctx, ctypes.byref(d), p, Bc.data_ptr(), ld(Bc), X.data_ptr(),
+                                      ld(X), cp, ldc, _prec_handle(N), ctypes.byref(opts),
+                                      ctypes.byref(st)), ctx)
+    stats = SimpleStats(st.niter, bool(st.solved),
+                        res[: min(st.n_residuals, len(res))].tolist() if history else [],
+                        st.timer, _status_string(st.status))
+    return X, stats

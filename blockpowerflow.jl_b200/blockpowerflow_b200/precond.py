@@ -1,0 +1,94 @@
+"""ILU(0) / IC(0) preconditioners: ilu0, ic0, ldiv! (src/preconditioners_nvidia.jl)."""
+from __future__ import annotations
+
+import ctypes as C
+
+from . import _lib
+from .sparse import CuSparseMatrixCSR, colmajor, empty_colmajor, ld
+
+
+class _DevicePrec:
+    kind = ""
+
+    def __init__(self, A: CuSparseMatrixCSR, nrhs: int, factor_dtype: str, creator: str):
+        self.A = A
+        self.n = A.n
+        self.nrhs = int(nrhs)
+        self.factor_dtype = factor_dtype
+        fd = _lib.BPF_F32 if factor_dtype in ("float32", "f32", "Float32") else _lib.BPF_F64
+        lib = _lib.load()
+        self._ctx = _lib.context(A.nzVal.device.index)
+        h = C.c_void_p()
+        d = A.desc()
+        _lib.check(getattr(lib, creator)(self._ctx, C.byref(d), self.nrhs, fd, C.byref(h)),
+                   self._ctx)
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def levels(self):
+        lo, up = C.c_int(), C.c_int()
+        _lib.check(_lib.load().bpf_prec_levels(self._h, C.byref(lo), C.byref(up)), self._ctx)
+        return lo.value, up.value
+
+    @property
+    def P(self):
+        """The factor values on A's pattern (NVIDIA_ILU0.P / NVIDIA_IC0.P)."""
+        import torch
+
+        v = torch.empty(self.A.nnz, dtype=torch.float64, device=self.A.nzVal.device)
+        _lib.check(_lib.load().bpf_prec_factor_values(self._h, v.data_ptr()), self._ctx)
+        return CuSparseMatrixCSR(self.A.rowPtr, self.A.colVal, v, self.n, self.A.index_base)
+
+    def refactor(self, vals) -> None:
+        """New values on the same pattern, then the numeric factorization again."""
+        _lib.check(_lib.load().bpf_prec_refactor(self._h, vals.data_ptr()), self._ctx)
+
+    def ldiv(self, x):
+        y = empty_colmajor(x.shape[0], 1 if x.dim() == 1 else x.shape[1], x.device)
+        ldiv_(y, self, x)
+        return y if x.dim() == 2 else y[:, 0]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.load().bpf_prec_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+class NVIDIA_ILU0(_DevicePrec):
+    kind = "ilu0"
+
+
+class NVIDIA_IC0(_DevicePrec):
+    kind = "ic0"
+
+
+def ilu0(A: CuSparseMatrixCSR, nrhs: int = 1, factor_dtype: str = "float64") -> NVIDIA_ILU0:
+    """ilu0(A, nrhs) (src/preconditioners_nvidia.jl:42-47)."""
+    return NVIDIA_ILU0(A, nrhs, factor_dtype, "bpf_ilu0_create")
+
+
+def ic0(A: CuSparseMatrixCSR, nrhs: int = 1, factor_dtype: str = "float64") -> NVIDIA_IC0:
+    """ic0(A, nrhs) (src/preconditioners_nvidia.jl:6-11)."""
+    return NVIDIA_IC0(A, nrhs, factor_dtype, "bpf_ic0_create")
+
+
+def ldiv_(y, P: _DevicePrec, x):
+    """ldiv!(y, P, x): y = P \\ x (vector or matrix x).  y must be a column-major block."""
+    vec = x.dim() == 1
+    xc = colmajor(x)
+    yc = y.reshape(-1, 1) if vec else y
+    n, p = xc.shape
+    if n != P.n or tuple(yc.shape) != (n, p):
+        raise _lib.DimensionMismatch(_lib.BPF_ERR_DIMENSION, "Inconsistent problem size")
+    if not (yc.stride(0) == 1):
+        raise ValueError("y must be column-major (Fortran order)")
+    _lib.check(_lib.load().bpf_prec_apply(P.handle, p, xc.data_ptr(), ld(xc), yc.data_ptr(),
+                                          ld(yc)), P._ctx)
+    return y

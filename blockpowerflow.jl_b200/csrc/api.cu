@@ -1,0 +1,376 @@
+// C ABI: context, errors, workspace, SpMM and preconditioner entry points.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "bpf_internal.cuh"
+#include "prec.cuh"
+
+namespace bpf {
+
+bpf_status set_error(bpf_ctx *ctx, bpf_status st, const char *fmt, ...) {
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        ctx->last_error = buf;
+    }
+    return st;
+}
+
+bpf_status cuda_error(bpf_ctx *ctx, cudaError_t e, const char *what, const char *file, int line) {
+    bpf_status st = (e == cudaErrorMemoryAllocation) ? BPF_ERR_ALLOC : BPF_ERR_CUDA;
+    return set_error(ctx, st, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+}
+
+void *ws_get(bpf_ctx *ctx, int slot, size_t bytes, bpf_status *st) {
+    *st = BPF_SUCCESS;
+    if (bytes == 0) bytes = 16;
+    if (ctx->ws_bytes[slot] >= bytes) return ctx->ws[slot];
+    if (ctx->ws[slot]) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->ws[slot]);
+        ctx->ws[slot] = nullptr;
+        ctx->ws_bytes[slot] = 0;
+    }
+    size_t want = bytes + bytes / 4;
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *st = set_error(ctx, BPF_ERR_ALLOC, "workspace allocation of %zu bytes failed: %s", want,
+                        cudaGetErrorString(e));
+        return nullptr;
+    }
+    ctx->ws[slot] = p;
+    ctx->ws_bytes[slot] = want;
+    return p;
+}
+
+bpf_status reset_dev_status(bpf_ctx *ctx) {
+    BPF_CUDA(ctx, cudaMemsetAsync(ctx->dstat, 0, sizeof(DevStatus), ctx->stream));
+    return BPF_SUCCESS;
+}
+
+bpf_status check_dev_status(bpf_ctx *ctx, const char *where) {
+    BPF_CUDA(ctx, cudaMemcpyAsync(ctx->hstat, ctx->dstat, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    int err = ctx->hstat->err, aux = ctx->hstat->aux;
+    if (err == DEV_OK) return BPF_SUCCESS;
+    // Clear the word (and the barrier state a timed-out barrier may have left) for the next call.
+    BPF_TRY(reset_dev_status(ctx));
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    switch (err) {
+        case DEV_ZERO_PIVOT:
+            return set_error(ctx, BPF_ERR_SINGULAR, "%s: zero pivot at row %d", where, aux);
+        case DEV_BARRIER_TIMEOUT:
+            return set_error(ctx, BPF_ERR_TIMEOUT, "%s: a device-side wait timed out", where);
+        case DEV_NONFINITE:
+            return set_error(ctx, BPF_ERR_NUMERIC, "%s: non-finite value at %d", where, aux);
+        case DEV_CHOL_FAIL:
+            return set_error(ctx, BPF_ERR_NUMERIC, "%s: Cholesky-QR breakdown", where);
+        default:
+            return set_error(ctx, BPF_ERR_CUDA, "%s: device error %d", where, err);
+    }
+}
+
+// Validate a CSR descriptor and copy its pattern to the host (0-based).
+bpf_status csr_pattern_to_host(bpf_ctx *ctx, const bpf_csr_desc *A, std::vector<int> &rp,
+                               std::vector<int> &ci, bool need_diag, std::vector<int> *diag) {
+    if (!A) return set_error(ctx, BPF_ERR_INVALID_VALUE, "null CSR descriptor");
+    if (A->n < 0 || A->nnz < 0 || (A->n > 0 && (!A->rowptr || (A->nnz > 0 && (!A->colind || !A->vals)))))
+        return set_error(ctx, BPF_ERR_INVALID_VALUE, "invalid CSR descriptor");
+    if (A->index_base != 0 && A->index_base != 1)
+        return set_error(ctx, BPF_ERR_INVALID_VALUE, "index_base must be 0 or 1");
+    int n = A->n, nnz = A->nnz, b = A->index_base;
+    rp.resize(n + 1);
+    ci.resize(nnz);
+    if (n > 0)
+        BPF_CUDA(ctx, cudaMemcpyAsync(rp.data(), A->rowptr, sizeof(int) * (n + 1),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    if (nnz > 0)
+        BPF_CUDA(ctx, cudaMemcpyAsync(ci.data(), A->colind, sizeof(int) * nnz,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (b) {
+        for (auto &v : rp) v -= b;
+        for (auto &v : ci) v -= b;
+    }
+    if (n > 0 && (rp[0] != 0 || rp[n] != nnz))
+        return set_error(ctx, BPF_ERR_INVALID_VALUE, "rowptr inconsistent with nnz=%d", nnz);
+    for (int i = 0; i < n; i++) {
+        if (rp[i + 1] < rp[i]) return set_error(ctx, BPF_ERR_INVALID_VALUE, "rowptr not monotone");
+        for (int k = rp[i]; k < rp[i + 1]; k++) {
+            if (ci[k] < 0 || ci[k] >= n)
+                return set_error(ctx, BPF_ERR_INVALID_VALUE, "column index out of range in row %d", i);
+            if (k > rp[i] && ci[k] <= ci[k - 1])
+                return set_error(ctx, BPF_ERR_INVALID_VALUE, "columns of row %d not sorted/unique", i);
+        }
+    }
+    if (need_diag) {
+        diag->assign(n, -1);
+        for (int i = 0; i < n; i++) {
+            for (int k = rp[i]; k < rp[i + 1]; k++)
+                if (ci[k] == i) { (*diag)[i] = k; break; }
+            if ((*diag)[i] < 0)
+                return set_error(ctx, BPF_ERR_SINGULAR, "structural zero pivot: A(%d,%d) missing", i, i);
+        }
+    }
+    return BPF_SUCCESS;
+}
+
+// Analyse a 0-based host pattern (sorted rows, diagonal present) and upload everything the
+// numeric factorization and the triangular solves need.  P->fv is allocated, not filled.
+// kind PREC_ILU0 / PREC_LU: unit L + U on the pattern; PREC_IC0: L and L' (lower part).
+bpf_status prec_setup(bpf_ctx *ctx, int kind, int n, const std::vector<int> &rp,
+                      const std::vector<int> &ci, const std::vector<int> &diag, bpf_prec **out) {
+    *out = nullptr;
+    const int nnz = n > 0 ? rp[n] : 0;
+    bpf_prec *P = new bpf_prec();
+    P->ctx = ctx;
+    P->kind = kind;
+    P->n = n;
+    P->nnz = nnz;
+    const bool ic = (kind == PREC_IC0);
+    TriHost lo = build_tri(n, rp.data(), ci.data(), diag.data(), 0, !ic);
+    TriHost up = ic ? build_tri(n, rp.data(), ci.data(), diag.data(), 2, false)
+                    : build_tri(n, rp.data(), ci.data(), diag.data(), 1, false);
+    std::vector<int> pp, pdst, psrc;
+    build_pairs(n, rp.data(), ci.data(), diag.data(), ic, pp, pdst, psrc);
+    P->npairs = (long long)pdst.size();
+    auto fail = [&](bpf_status s) {
+        cudaStreamSynchronize(ctx->stream);
+        bpf_prec_destroy(P);
+        return s;
+    };
+    bpf_status s;
+    if ((s = tri_upload(ctx, lo, P->lower)) != BPF_SUCCESS) return fail(s);
+    if ((s = tri_upload(ctx, up, P->upper)) != BPF_SUCCESS) return fail(s);
+    cudaError_t e = cudaSuccess;
+    auto up_i = [&](int **d, const std::vector<int> &h) {
+        if (e != cudaSuccess || h.empty()) return;
+        e = cudaMalloc((void **)d, sizeof(int) * h.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(*d, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, ctx->stream);
+    };
+    up_i(&P->rp, rp);
+    up_i(&P->ci, ci);
+    up_i(&P->diag, diag);
+    up_i(&P->pp, pp);
+    up_i(&P->pdst, pdst);
+    up_i(&P->psrc, psrc);
+    if (e == cudaSuccess && nnz > 0) e = cudaMalloc((void **)&P->fv, sizeof(double) * nnz);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // host vectors die on return
+    if (e != cudaSuccess) return fail(cuda_error(ctx, e, "preconditioner setup", __FILE__, __LINE__));
+    *out = P;
+    return BPF_SUCCESS;
+}
+
+}  // namespace bpf
+
+using namespace bpf;
+
+extern "C" {
+
+bpf_status bpf_ctx_create(bpf_ctx **out, void *stream) {
+    if (!out) return BPF_ERR_INVALID_VALUE;
+    *out = nullptr;
+    bpf_ctx *ctx = new bpf_ctx();
+    ctx->stream = (cudaStream_t)stream;
+    cudaError_t e = cudaGetDevice(&ctx->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&ctx->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&ctx->dstat, sizeof(DevStatus));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->hstat, sizeof(DevStatus));
+    if (e == cudaSuccess) e = cudaMemset(ctx->dstat, 0, sizeof(DevStatus));
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (ctx->dstat) cudaFree(ctx->dstat);
+        if (ctx->hstat) cudaFreeHost(ctx->hstat);
+        delete ctx;
+        return e == cudaErrorMemoryAllocation ? BPF_ERR_ALLOC : BPF_ERR_CUDA;
+    }
+    *out = ctx;
+    return BPF_SUCCESS;
+}
+
+bpf_status bpf_ctx_set_stream(bpf_ctx *ctx, void *stream) {
+    if (!ctx) return BPF_ERR_INVALID_VALUE;
+    ctx->stream = (cudaStream_t)stream;
+    return BPF_SUCCESS;
+}
+
+bpf_status bpf_ctx_destroy(bpf_ctx *ctx) {
+    if (!ctx) return BPF_SUCCESS;
+    cudaStreamSynchronize(ctx->stream);
+    for (int s = 0; s < WS_COUNT; s++)
+        if (ctx->ws[s]) cudaFree(ctx->ws[s]);
+    cudaFree(ctx->dstat);
+    cudaFreeHost(ctx->hstat);
+    delete ctx;
+    return BPF_SUCCESS;
+}
+
+const char *bpf_last_error(const bpf_ctx *ctx) {
+    if (!ctx) return "null context";
+    return ctx->last_error.c_str();
+}
+
+long long bpf_ctx_kernel_launches(const bpf_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+const char *bpf_solve_status_string(int status) {
+    switch (status) {
+        case BPF_SOLVE_SOLVED: return "solution good enough given atol and rtol";
+        case BPF_SOLVE_ITMAX: return "maximum number of iterations exceeded";
+        case BPF_SOLVE_TIMEMAX: return "time limit exceeded";
+        default: return "unknown";
+    }
+}
+
+bpf_status bpf_spmm(bpf_ctx *ctx, const bpf_csr_desc *A, int p, double alpha, const double *X,
+                    int ldx, double beta, double *Y, int ldy) {
+    if (!ctx) return BPF_ERR_INVALID_VALUE;
+    if (!A || p < 0 || (p > 0 && A->n > 0 && (!X || !Y)))
+        return set_error(ctx, BPF_ERR_INVALID_VALUE, "bpf_spmm: invalid argument");
+    if (A->dtype != BPF_F64) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "bpf_spmm: FP64 matrices only");
+    int n = A->n;
+    if (ldx < std::max(1, n) || ldy < std::max(1, n))
+        return set_error(ctx, BPF_ERR_DIMENSION, "bpf_spmm: leading dimension < n");
+    if (n == 0 || p == 0) return BPF_SUCCESS;
+    bpf_status st;
+    const int chunk = 256;
+    size_t cols = std::min(p, chunk);
+    double *xr = (double *)ws_get(ctx, WS_A, sizeof(double) * (size_t)n * cols, &st);
+    if (!xr) return st;
+    double *yr = (double *)ws_get(ctx, WS_B, sizeof(double) * (size_t)n * cols, &st);
+    if (!yr) return st;
+    for (int c0 = 0; c0 < p; c0 += chunk) {
+        int pc = std::min(chunk, p - c0);
+        BPF_TRY(colmajor_to_rowmajor(ctx, n, pc, X + (size_t)c0 * ldx, ldx, xr));
+        if (beta != 0.0) BPF_TRY(colmajor_to_rowmajor(ctx, n, pc, Y + (size_t)c0 * ldy, ldy, yr));
+        BPF_TRY(spmm_rowmajor(ctx, n, A->rowptr, A->colind, (const double *)A->vals, A->index_base,
+                              pc, alpha, xr, beta, yr, nullptr));
+        BPF_TRY(rowmajor_to_colmajor(ctx, n, pc, yr, Y + (size_t)c0 * ldy, ldy));
+    }
+    return BPF_SUCCESS;
+}
+
+static bpf_status prec_create(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs, int fdtype,
+                              int kind, bpf_prec **out) {
+    if (!ctx || !out) return BPF_ERR_INVALID_VALUE;
+    *out = nullptr;
+    if (!A) return set_error(ctx, BPF_ERR_INVALID_VALUE, "null matrix");
+    if (A->dtype != BPF_F64) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "FP64 matrices only");
+    if (fdtype != BPF_F64 && fdtype != BPF_F32)
+        return set_error(ctx, BPF_ERR_INVALID_VALUE, "factor dtype must be BPF_F64 or BPF_F32");
+    std::vector<int> rp, ci, diag;
+    BPF_TRY(csr_pattern_to_host(ctx, A, rp, ci, true, &diag));
+    int n = A->n, nnz = A->nnz;
+    bpf_prec *P = nullptr;
+    BPF_TRY(prec_setup(ctx, kind, n, rp, ci, diag, &P));
+    P->nrhs = nrhs;
+    P->fdtype = fdtype;
+    bool ic = (kind == PREC_IC0);
+    auto fail = [&](bpf_status s) {
+        cudaStreamSynchronize(ctx->stream);
+        bpf_prec_destroy(P);
+        return s;
+    };
+    bpf_status s;
+    if (nnz > 0) {
+        cudaError_t e = cudaMemcpyAsync(P->fv, A->vals, sizeof(double) * nnz, cudaMemcpyDeviceToDevice,
+                                        ctx->stream);
+        if (e != cudaSuccess) return fail(cuda_error(ctx, e, "preconditioner setup", __FILE__, __LINE__));
+    }
+    if ((s = factor_numeric(ctx, P)) != BPF_SUCCESS) return fail(s);
+    if ((s = tri_scatter(ctx, P->lower, P->fv)) != BPF_SUCCESS) return fail(s);
+    if ((s = tri_scatter(ctx, P->upper, P->fv)) != BPF_SUCCESS) return fail(s);
+    if ((s = check_dev_status(ctx, ic ? "ic0" : "ilu0")) != BPF_SUCCESS) return fail(s);
+    *out = P;
+    return BPF_SUCCESS;
+}
+
+bpf_status bpf_ilu0_create(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs, int factor_dtype,
+                           bpf_prec **prec) {
+    return prec_create(ctx, A, nrhs, factor_dtype, PREC_ILU0, prec);
+}
+
+bpf_status bpf_ic0_create(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs, int factor_dtype,
+                          bpf_prec **prec) {
+    return prec_create(ctx, A, nrhs, factor_dtype, PREC_IC0, prec);
+}
+
+bpf_status bpf_prec_refactor(bpf_prec *P, const double *vals) {
+    if (!P) return BPF_ERR_INVALID_VALUE;
+    bpf_ctx *ctx = P->ctx;
+    if (P->nnz > 0 && !vals) return set_error(ctx, BPF_ERR_INVALID_VALUE, "null values");
+    if (P->nnz > 0)
+        BPF_CUDA(ctx, cudaMemcpyAsync(P->fv, vals, sizeof(double) * P->nnz, cudaMemcpyDeviceToDevice,
+                                      ctx->stream));
+    BPF_TRY(factor_numeric(ctx, P));
+    BPF_TRY(tri_scatter(ctx, P->lower, P->fv));
+    BPF_TRY(tri_scatter(ctx, P->upper, P->fv));
+    return check_dev_status(ctx, P->kind == PREC_IC0 ? "ic0 refactor" : "ilu0 refactor");
+}
+
+bpf_status bpf_prec_apply(bpf_prec *P, int p, const double *X, int ldx, double *Y, int ldy) {
+    if (!P) return BPF_ERR_INVALID_VALUE;
+    bpf_ctx *ctx = P->ctx;
+    int n = P->n;
+    if (p < 0 || (p > 0 && n > 0 && (!X || !Y)))
+        return set_error(ctx, BPF_ERR_INVALID_VALUE, "bpf_prec_apply: invalid argument");
+    if (ldx < std::max(1, n) || ldy < std::max(1, n))
+        return set_error(ctx, BPF_ERR_DIMENSION, "bpf_prec_apply: leading dimension < n");
+    if (n == 0 || p == 0) return BPF_SUCCESS;
+    const int chunk = 256;
+    bpf_status st;
+    double *buf = (double *)ws_get(ctx, WS_A, sizeof(double) * (size_t)n * std::min(p, chunk), &st);
+    if (!buf) return st;
+    for (int c0 = 0; c0 < p; c0 += chunk) {
+        int pc = std::min(chunk, p - c0);
+        BPF_TRY(colmajor_to_rowmajor(ctx, n, pc, X + (size_t)c0 * ldx, ldx, buf));
+        BPF_TRY(prec_apply_rowmajor(ctx, P, pc, buf, buf));
+        BPF_TRY(rowmajor_to_colmajor(ctx, n, pc, buf, Y + (size_t)c0 * ldy, ldy));
+    }
+    return BPF_SUCCESS;
+}
+
+bpf_status bpf_prec_factor_values(const bpf_prec *P, double *vals) {
+    if (!P || (P->nnz > 0 && !vals)) return BPF_ERR_INVALID_VALUE;
+    bpf_ctx *ctx = P->ctx;
+    if (P->nnz > 0)
+        BPF_CUDA(ctx, cudaMemcpyAsync(vals, P->fv, sizeof(double) * P->nnz, cudaMemcpyDeviceToDevice,
+                                      ctx->stream));
+    return BPF_SUCCESS;
+}
+
+bpf_status bpf_prec_levels(const bpf_prec *P, int *lo, int *up) {
+    if (!P) return BPF_ERR_INVALID_VALUE;
+    if (lo) *lo = P->lower.nlev;
+    if (up) *up = P->upper.nlev;
+    return BPF_SUCCESS;
+}
+
+bpf_status bpf_prec_destroy(bpf_prec *P) {
+    if (!P) return BPF_SUCCESS;
+    if (P->ctx) cudaStreamSynchronize(P->ctx->stream);
+    tri_free(P->lower);
+    tri_free(P->upper);
+    cudaFree(P->rp);
+    cudaFree(P->ci);
+    cudaFree(P->diag);
+    cudaFree(P->pp);
+    cudaFree(P->pdst);
+    cudaFree(P->psrc);
+    cudaFree(P->fv);
+    delete P;
+    return BPF_SUCCESS;
+}
+
+}  // extern "C"

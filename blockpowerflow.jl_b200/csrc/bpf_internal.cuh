@@ -1,0 +1,202 @@
+// Internal definitions shared by the libbpf translation units (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/bpf.h"
+
+namespace bpf {
+
+// ------------------------------------------------------------------------------------
+// device-side error word (one per context)
+// ------------------------------------------------------------------------------------
+enum DevErr : int {
+    DEV_OK = 0,
+    DEV_ZERO_PIVOT = 1,      // factorization met a zero / non-positive pivot (row in aux)
+    DEV_BARRIER_TIMEOUT = 2, // a bounded grid-barrier wait gave up
+    DEV_NONFINITE = 3,       // NaN/Inf residual
+    DEV_CHOL_FAIL = 4,       // Cholesky-QR Gram matrix not positive definite
+};
+
+struct DevStatus {
+    int err;        // DevErr
+    int aux;        // row / column index for diagnostics
+    unsigned bar_count;  // grid barrier arrival counter
+    unsigned bar_gen;    // grid barrier generation
+    int pad[4];
+};
+
+// Workspace slots held by a context (grow-only, reused across calls).
+enum Slot : int {
+    WS_PARTIAL = 0,   // split-K partial sums of Gram products
+    WS_SMALL,         // p x p scratch matrices
+    WS_A,
+    WS_B,
+    WS_C,
+    WS_D,
+    WS_E,
+    WS_F,
+    WS_G,
+    WS_H,
+    WS_V,             // Krylov basis
+    WS_HESS,          // packed R blocks of the block Hessenberg QR
+    WS_STATE,         // solver state struct
+    WS_HIST,          // residual history
+    WS_I32,
+    WS_NORM,          // reduction partials
+    WS_Z,             // least-squares right-hand side blocks
+    WS_HY,            // Householder reflectors (2p x p) and T factors per block column
+    WS_HSCR,          // scratch of the one-CTA small-matrix kernels
+    WS_VEC,           // n x p working blocks of a solve
+    WS_COUNT
+};
+
+}  // namespace bpf
+
+struct bpf_ctx {
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    int num_sms = 148;
+    int max_smem_optin = 0;
+    std::string last_error;
+    long long launches = 0;
+    bpf::DevStatus *dstat = nullptr;   // device
+    bpf::DevStatus *hstat = nullptr;   // pinned host mirror
+    void *ws[bpf::WS_COUNT] = {};
+    size_t ws_bytes[bpf::WS_COUNT] = {};
+};
+
+namespace bpf {
+
+// ------------------------------------------------------------------------------------
+// host-side error helpers
+// ------------------------------------------------------------------------------------
+bpf_status set_error(bpf_ctx *ctx, bpf_status st, const char *fmt, ...);
+bpf_status cuda_error(bpf_ctx *ctx, cudaError_t e, const char *what, const char *file, int line);
+void *ws_get(bpf_ctx *ctx, int slot, size_t bytes, bpf_status *st);
+bpf_status check_dev_status(bpf_ctx *ctx, const char *where);
+bpf_status reset_dev_status(bpf_ctx *ctx);
+
+#define BPF_CUDA(ctx, call)                                                          \
+    do {                                                                             \
+        cudaError_t _e = (call);                                                     \
+        if (_e != cudaSuccess) return ::bpf::cuda_error(ctx, _e, #call, __FILE__, __LINE__); \
+    } while (0)
+
+#define BPF_LAUNCHED(ctx)                                                            \
+    do {                                                                             \
+        (ctx)->launches++;                                                           \
+        cudaError_t _e = cudaGetLastError();                                         \
+        if (_e != cudaSuccess) return ::bpf::cuda_error(ctx, _e, "kernel launch", __FILE__, __LINE__); \
+    } while (0)
+
+#define BPF_TRY(expr)                                                                \
+    do {                                                                             \
+        bpf_status _s = (expr);                                                      \
+        if (_s != BPF_SUCCESS) return _s;                                            \
+    } while (0)
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// ------------------------------------------------------------------------------------
+// device helpers
+// ------------------------------------------------------------------------------------
+#ifdef __CUDACC__
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_sumf(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ int ld_relaxed_i32(const int *p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Spin limit of every cross-CTA wait: ~2^21 polls with a short sleep each (about a second),
+// after which the wait records DEV_BARRIER_TIMEOUT and returns.
+constexpr long long kSpinLimit = 1LL << 21;
+
+// Grid-wide barrier for a cooperative (co-resident) launch.  `gen` is the generation the
+// calling block last saw (read once at kernel start by thread 0 of each block).  Returns
+// false (in every thread of the block) if the barrier timed out or an error is pending, in
+// which case the caller must return without further global writes.
+__device__ __forceinline__ bool grid_barrier(DevStatus *ds, unsigned &gen) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (gridDim.x == 1) {
+        return true;
+    }
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        unsigned g = gen;
+        __threadfence();
+        unsigned prev = atomicAdd(&ds->bar_count, 1u);
+        if (prev == gridDim.x - 1) {
+            atomicExch(&ds->bar_count, 0u);
+            __threadfence();
+            st_release_u32(&ds->bar_gen, g + 1);
+        } else {
+            long long it = 0;
+            while (ld_acquire_u32(&ds->bar_gen) == g) {
+                if (++it > kSpinLimit || ld_relaxed_i32(&ds->err) != 0) {
+                    ok = 0;
+                    atomicCAS(&ds->err, 0, (int)DEV_BARRIER_TIMEOUT);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        gen = g + 1;
+        if (ld_relaxed_i32(&ds->err) != 0) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+__device__ __forceinline__ unsigned barrier_gen_start(DevStatus *ds) {
+    return ld_acquire_u32(&ds->bar_gen);
+}
+#endif
+
+// ------------------------------------------------------------------------------------
+// launchers implemented in the .cu files
+// ------------------------------------------------------------------------------------
+// Column-major (ld) <-> row-major (n x p, ld = p) block conversions.
+bpf_status colmajor_to_rowmajor(bpf_ctx *ctx, int n, int p, const double *src, int ld,
+                                double *dst);
+bpf_status rowmajor_to_colmajor(bpf_ctx *ctx, int n, int p, const double *src, double *dst,
+                                int ld);
+
+// CSR SpMM on row-major blocks: Y = alpha*A*X + beta*Y, or (residual) Y = B - A*X when
+// B != nullptr.  base = index base of the CSR arrays.
+bpf_status spmm_rowmajor(bpf_ctx *ctx, int n, const int *rp, const int *ci, const double *av,
+                         int base, int p, double alpha, const double *X, double beta,
+                         double *Y, const double *B, const int *gate = nullptr);
+// Same with an FP32 input block (mixed-precision path): Y = A*X.
+bpf_status spmm_rowmajor_f32x(bpf_ctx *ctx, int n, const int *rp, const int *ci,
+                              const double *av, int base, int p, const float *X, double *Y,
+                              const int *gate = nullptr);
+
+}  // namespace bpf

@@ -1,0 +1,544 @@
+// Dense block kernels: Gram products, tall x small products, Cholesky-QR, reductions.
+//
+// They replace the cuBLAS gemm / nrm2 / dot and cuSOLVER geqrf / orgqr calls the reference
+// makes on n x p blocks (src/block_gmres.jl:301-316, src/block_utils.jl:46-53,
+// src/block_bicgstab.jl:136-153).  FP64 throughout (B200 runs FP64 FMA and FP64 MMA at the
+// same rate, so the FMA path with shared-memory tiles is used).
+//
+//  gram : Out_j = A_j^T B, split over rows into chunks (grid.x), one p x p tile per CTA,
+//         partial sums reduced by a second deterministic kernel.
+//         Algorithmic bytes: 8*n*p*(nb + 1); flops 2*n*p*p*nb.
+//  tsmm : Out = beta*C + alpha*sum_j A_j S_j, one 64-row x 64-column tile per CTA.
+//         Algorithmic bytes: 8*n*p*(nb + 1 [+1 for C]); flops 2*n*p*p*nb.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "bpf_internal.cuh"
+#include "dense.cuh"
+
+namespace bpf {
+
+constexpr int kGramRows = 32;   // rows per shared-memory stage of gram
+constexpr int kTsmmRows = 64;   // rows per CTA of tsmm
+constexpr int kTsmmK = 16;      // inner-dimension stage of tsmm
+
+__device__ __forceinline__ bool gate_off(const SolveState *st, const int *gate,
+                                         const int *gate2 = nullptr) {
+    if (st && !st->active) return true;
+    if (gate && *gate == 0) return true;
+    if (gate2 && *gate2 == 0) return true;
+    return false;
+}
+
+// ---------------------------------------------------------------------------------------
+// gram
+// ---------------------------------------------------------------------------------------
+template <int GT>
+__global__ void __launch_bounds__(256)
+gram_partial_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
+                    const double *__restrict__ B, double *__restrict__ partial,
+                    int rows_per_chunk, const SolveState *st, const int *gate,
+                    const int *gate2) {
+    if (gate_off(st, gate, gate2)) return;
+    constexpr int TPD = GT / 16;   // outputs per thread per dimension
+    __shared__ double As[kGramRows][GT];
+    __shared__ double Bs[kGramRows][GT];
+    const int chunk = blockIdx.x, j = blockIdx.y;
+    const int ntile = (p + GT - 1) / GT;
+    const int a0 = (blockIdx.z / ntile) * GT, b0 = (blockIdx.z % ntile) * GT;
+    const int r_begin = chunk * rows_per_chunk;
+    const int r_end = min(n, r_begin + rows_per_chunk);
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const double *Aj = A + (size_t)j * strideA;
+    double acc[TPD][TPD];
+#pragma unroll
+    for (int i = 0; i < TPD; i++)
+#pragma unroll
+        for (int k = 0; k < TPD; k++) acc[i][k] = 0.0;
+    for (int r0 = r_begin; r0 < r_end; r0 += kGramRows) {
+        for (int e = threadIdx.x; e < kGramRows * GT; e += 256) {
+            const int rr = e / GT, cc = e % GT, r = r0 + rr;
+            const bool rok = r < r_end;
+            As[rr][cc] = (rok && a0 + cc < p) ? __ldg(Aj + (size_t)r * p + a0 + cc) : 0.0;
+            Bs[rr][cc] = (rok && b0 + cc < p) ? __ldg(B + (size_t)r * p + b0 + cc) : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int rr = 0; rr < kGramRows; rr++) {
+            double a[TPD], b[TPD];
+#pragma unroll
+            for (int i = 0; i < TPD; i++) a[i] = As[rr][ty + 16 * i];
+#pragma unroll
+            for (int k = 0; k < TPD; k++) b[k] = Bs[rr][tx + 16 * k];
+#pragma unroll
+            for (int i = 0; i < TPD; i++)
+#pragma unroll
+                for (int k = 0; k < TPD; k++) acc[i][k] = fma(a[i], b[k], acc[i][k]);
+        }
+        __syncthreads();
+    }
+    double *out = partial + ((size_t)chunk * nb + j) * p * p;
+#pragma unroll
+    for (int i = 0; i < TPD; i++) {
+        const int a = a0 + ty + 16 * i;
+        if (a >= p) continue;
+#pragma unroll
+        for (int k = 0; k < TPD; k++) {
+            const int b = b0 + tx + 16 * k;
+            if (b < p) out[(size_t)a * p + b] = acc[i][k];
+        }
+    }
+}
+
+__global__ void gram_reduce_kernel(int total, int nchunks, const double *__restrict__ partial,
+                                   double *__restrict__ out, double alpha, int accumulate,
+                                   double *__restrict__ out2, const SolveState *st,
+                                   const int *gate, const int *gate2) {
+    if (gate_off(st, gate, gate2)) return;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < nchunks; c++) s += partial[(size_t)c * total + e];
+        s *= alpha;
+        if (out2) out2[e] = s;
+        if (accumulate) s += out[e];
+        out[e] = s;
+    }
+}
+
+bpf_status gram(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t strideA,
+                const double *B, double *Out, double alpha, bool accumulate,
+                const SolveState *st, const int *qr_gate, double *Out2, const int *gate2) {
+    if (nb <= 0 || p <= 0) return BPF_SUCCESS;
+    const int GT = p <= 16 ? 16 : (p <= 32 ? 32 : 64);
+    const int ntile = ceil_div(p, GT);
+    const int tiles = ntile * ntile;
+    const int target = ctx->num_sms * 4;
+    int nchunks = std::max(1, std::min(ceil_div(n, kGramRows), target / std::max(1, nb * tiles)));
+    int rows_per_chunk = ceil_div(std::max(n, 1), nchunks);
+    rows_per_chunk = ceil_div(rows_per_chunk, kGramRows) * kGramRows;
+    nchunks = std::max(1, ceil_div(std::max(n, 1), rows_per_chunk));
+    bpf_status s;
+    double *partial = (double *)ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)nchunks * nb * p * p, &s);
+    if (!partial) return s;
+    dim3 grid(nchunks, nb, tiles);
+    if (GT == 16)
+        gram_partial_kernel<16><<<grid, 256, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
+                                                                rows_per_chunk, st, qr_gate, gate2);
+    else if (GT == 32)
+        gram_partial_kernel<32><<<grid, 256, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
+                                                                rows_per_chunk, st, qr_gate, gate2);
+    else
+        gram_partial_kernel<64><<<grid, 256, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
+                                                                rows_per_chunk, st, qr_gate, gate2);
+    BPF_LAUNCHED(ctx);
+    int total = nb * p * p;
+    int blocks = std::min(ceil_div(total, 256), ctx->num_sms * 4);
+    gram_reduce_kernel<<<blocks, 256, 0, ctx->stream>>>(total, nchunks, partial, Out, alpha,
+                                                         accumulate ? 1 : 0, Out2, st, qr_gate, gate2);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------------------
+// tsmm
+// ---------------------------------------------------------------------------------------
+template <int GT>
+__global__ void __launch_bounds__(256)
+tsmm_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
+            const double *__restrict__ S, size_t strideS, double alpha, const double *Cin,
+            double beta, double *Out, const SolveState *st, const int *nb_dev, const int *gate,
+            const int *gate2) {
+    if (gate_off(st, gate, gate2)) return;
+    constexpr int TPD = GT / 16;
+    constexpr int RPT = kTsmmRows / 16;
+    __shared__ double As[kTsmmRows][kTsmmK + 1];
+    __shared__ double Ss[kTsmmK][GT];
+    const int r0 = blockIdx.x * kTsmmRows;
+    const int b0 = blockIdx.y * GT;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    int nbl = nb;
+    if (nb_dev) nbl = min(nb, *nb_dev);
+    double acc[RPT][TPD];
+#pragma unroll
+    for (int i = 0; i < RPT; i++)
+#pragma unroll
+        for (int k = 0; k < TPD; k++) acc[i][k] = 0.0;
+    for (int j = 0; j < nbl; j++) {
+        const double *Aj = A + (size_t)j * strideA;
+        const double *Sj = S + (size_t)j * strideS;
+        for (int k0 = 0; k0 < p; k0 += kTsmmK) {
+            for (int e = threadIdx.x; e < kTsmmRows * kTsmmK; e += 256) {
+                const int rr = e / kTsmmK, kk = e % kTsmmK;
+                const int r = r0 + rr, c = k0 + kk;
+                As[rr][kk] = (r < n && c < p) ? __ldg(Aj + (size_t)r * p + c) : 0.0;
+            }
+            for (int e = threadIdx.x; e < kTsmmK * GT; e += 256) {
+                const int kk = e / GT, cc = e % GT;
+                const int a = k0 + kk, b = b0 + cc;
+                Ss[kk][cc] = (a < p && b < p) ? __ldg(Sj + (size_t)a * p + b) : 0.0;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < kTsmmK; kk++) {
+                double a[RPT], b[TPD];
+#pragma unroll
+                for (int i = 0; i < RPT; i++) a[i] = As[ty + 16 * i][kk];
+#pragma unroll
+                for (int k = 0; k < TPD; k++) b[k] = Ss[kk][tx + 16 * k];
+#pragma unroll
+                for (int i = 0; i < RPT; i++)
+#pragma unroll
+                    for (int k = 0; k < TPD; k++) acc[i][k] = fma(a[i], b[k], acc[i][k]);
+            }
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < RPT; i++) {
+        const int r = r0 + ty + 16 * i;
+        if (r >= n) continue;
+#pragma unroll
+        for (int k = 0; k < TPD; k++) {
+            const int b = b0 + tx + 16 * k;
+            if (b >= p) continue;
+            double v = alpha * acc[i][k];
+            if (Cin && beta != 0.0) v += beta * Cin[(size_t)r * p + b];
+            Out[(size_t)r * p + b] = v;
+        }
+    }
+}
+
+bpf_status tsmm(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t strideA,
+                const double *S, size_t strideS, double alpha, const double *Cin, double beta,
+                double *Out, const SolveState *st, const int *nb_dev, const int *qr_gate,
+                const int *gate2) {
+    if (n <= 0 || p <= 0) return BPF_SUCCESS;
+    const int GT = p <= 16 ? 16 : (p <= 32 ? 32 : 64);
+    dim3 grid(ceil_div(n, kTsmmRows), ceil_div(p, GT));
+    if (GT == 16)
+        tsmm_kernel<16><<<grid, 256, 0, ctx->stream>>>(n, p, nb, A, strideA, S, strideS, alpha, Cin,
+                                                        beta, Out, st, nb_dev, qr_gate, gate2);
+    else if (GT == 32)
+        tsmm_kernel<32><<<grid, 256, 0, ctx->stream>>>(n, p, nb, A, strideA, S, strideS, alpha, Cin,
+                                                        beta, Out, st, nb_dev, qr_gate, gate2);
+    else
+        tsmm_kernel<64><<<grid, 256, 0, ctx->stream>>>(n, p, nb, A, strideA, S, strideS, alpha, Cin,
+                                                        beta, Out, st, nb_dev, qr_gate, gate2);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------------------
+// Cholesky of the Gram matrix (one CTA): G = R^T R, R upper; Rinv = R^{-1};
+// Racc <- R * Racc (or R when first).  pass 0 may shift G (Fukaya et al., shifted CholeskyQR:
+// s = 11 (n p + p (p+1)) u ||G||, ||G|| bounded by trace(G)) when a pivot falls below
+// 1e-13 of the column's original norm; it then sets st->qr_shift so the third pass runs.
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024)
+chol_kernel(int n, int p, const double *__restrict__ G, double *__restrict__ Rinv,
+            double *__restrict__ Racc, double *__restrict__ Rtmp, int pass, SolveState *st,
+            const int *gate, const int *gate2, int *shift_flag, int *reorth_flag, DevStatus *ds) {
+    if (st && !st->active) return;
+    if (gate && *gate == 0) return;
+    if (gate2 && *gate2 == 0) return;
+    extern __shared__ double g[];            // p*p
+    __shared__ int s_fail;
+    __shared__ double s_shift;
+    __shared__ double s_minratio;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int pp = p * p;
+    if (pass == 0 && tid == 0 && shift_flag) *shift_flag = 0;
+    if (tid == 0) s_minratio = 1.0;
+    double trace = 0.0;
+    for (int i = 0; i < p; i++) trace += G[i * p + i];
+    for (int attempt = 0; attempt < 2; attempt++) {
+        if (tid == 0) {
+            s_fail = 0;
+            s_shift = attempt == 0 ? 0.0
+                                   : 11.0 * ((double)n * p + (double)p * (p + 1)) * 1.1102230246251565e-16 * trace;
+        }
+        __syncthreads();
+        for (int e = tid; e < pp; e += nt) g[e] = G[e] + ((e / p == e % p) ? s_shift : 0.0);
+        __syncthreads();
+        for (int j = 0; j < p; j++) {
+            if (tid == 0) {
+                double d = g[j * p + j];
+                double ref = G[j * p + j] + s_shift;
+                if (attempt == 0) s_minratio = fmin(s_minratio, (ref > 0.0) ? d / ref : 0.0);
+                if (!(d > 1e-13 * ref) || !(d > 0.0)) {
+                    s_fail = 1;
+                } else {
+                    g[j * p + j] = sqrt(d);
+                }
+            }
+            __syncthreads();
+            if (s_fail) break;
+            const double inv = 1.0 / g[j * p + j];
+            for (int c = j + 1 + tid; c < p; c += nt) g[j * p + c] *= inv;
+            __syncthreads();
+            const int m = p - j - 1;
+            for (int e = tid; e < m * m; e += nt) {
+                const int a = j + 1 + e / m, b = j + 1 + e % m;
+                if (b >= a) g[a * p + b] -= g[j * p + a] * g[j * p + b];
+            }
+            __syncthreads();
+        }
+        if (attempt == 0 && tid == 0 && pass == 0 && reorth_flag)
+            *reorth_flag = (s_fail || s_minratio < 1e-8) ? 1 : 0;
+        if (!s_fail) break;
+        if (attempt == 0 && shift_flag) {
+            if (tid == 0) *shift_flag = 1;
+        }
+        __syncthreads();
+    }
+    if (s_fail) {
+        if (tid == 0) {
+            if (st) st->qr_fail = 1;
+            if (ds && atomicCAS(&ds->err, 0, (int)DEV_CHOL_FAIL) == 0) ds->aux = pass;
+        }
+        return;
+    }
+    // zero the strict lower triangle so g holds R
+    for (int e = tid; e < pp; e += nt)
+        if (e / p > e % p) g[e] = 0.0;
+    __syncthreads();
+    // Rinv: warp w solves R x = e_c for columns c = w, w+nwarps, ...
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    for (int c = warp; c < p; c += nwarps) {
+        double b[4];
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const int r = lane + 32 * t;
+            b[t] = (r == c) ? 1.0 : 0.0;
+        }
+        for (int k = c; k >= 0; k--) {
+            const int owner = k & 31, slot = k >> 5;
+            double bk = 0.0;
+#pragma unroll
+            for (int t = 0; t < 4; t++)
+                if (t == slot) bk = b[t];
+            bk = __shfl_sync(0xffffffffu, bk, owner);
+            const double xk = bk / g[k * p + k];
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const int r = lane + 32 * t;
+                if (r == k) b[t] = xk;
+                else if (r < k) b[t] -= g[r * p + k] * xk;
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const int r = lane + 32 * t;
+            if (r < p) Rinv[r * p + c] = (r <= c) ? b[t] : 0.0;
+        }
+    }
+    // Racc <- R * Racc (pass > 0) or R (pass 0)
+    if (pass == 0) {
+        for (int e = tid; e < pp; e += nt) Racc[e] = g[e];
+    } else {
+        for (int e = tid; e < pp; e += nt) {
+            const int a = e / p, b = e % p;
+            double s = 0.0;
+            for (int c = a; c <= b; c++) s += g[a * p + c] * Racc[c * p + b];
+            Rtmp[e] = (b >= a) ? s : 0.0;
+        }
+        __syncthreads();
+        for (int e = tid; e < pp; e += nt) Racc[e] = Rtmp[e];
+    }
+}
+
+__global__ void gated_copy_kernel(size_t len, const double *__restrict__ src,
+                                  double *__restrict__ dst, const SolveState *st, const int *gate,
+                                  const int *gate2) {
+    if (gate_off(st, gate, gate2)) return;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < len;
+         e += (size_t)gridDim.x * blockDim.x)
+        dst[e] = src[e];
+}
+
+static bpf_status launch_chol(bpf_ctx *ctx, int n, int p, const double *G, double *Rinv,
+                              double *Racc, double *Rtmp, int pass, SolveState *st,
+                              const int *gate, const int *gate2, int *shift_flag,
+                              int *reorth_flag) {
+    size_t smem = sizeof(double) * p * p;
+    if (smem > 48 * 1024) {
+        BPF_CUDA(ctx, cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+    }
+    chol_kernel<<<1, 1024, smem, ctx->stream>>>(n, p, G, Rinv, Racc, Rtmp, pass, st, gate, gate2,
+                                                shift_flag, reorth_flag, ctx->dstat);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+bpf_status cholqr(bpf_ctx *ctx, int n, int p, const double *W, double *Q, double *R,
+                  double *T, SolveState *st, const int *gate, int *shift_flag, int *reorth_flag) {
+    if (p > 128) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "Cholesky-QR: p=%d > 128", p);
+    bpf_status s;
+    double *small = (double *)ws_get(ctx, WS_SMALL, sizeof(double) * 3 * p * p, &s);
+    if (!small) return s;
+    double *G = small, *Rinv = small + p * p, *Rtmp = small + 2 * p * p;
+    if (!shift_flag) shift_flag = &st->qr_shift;
+    const int *g3 = shift_flag;
+    // pass 1: W -> T
+    BPF_TRY(gram(ctx, n, p, 1, W, 0, W, G, 1.0, false, st, gate));
+    BPF_TRY(launch_chol(ctx, n, p, G, Rinv, R, Rtmp, 0, st, gate, nullptr, shift_flag, reorth_flag));
+    BPF_TRY(tsmm(ctx, n, p, 1, W, 0, Rinv, 0, 1.0, nullptr, 0.0, T, st, nullptr, gate));
+    // pass 2: T -> Q
+    BPF_TRY(gram(ctx, n, p, 1, T, 0, T, G, 1.0, false, st, gate));
+    BPF_TRY(launch_chol(ctx, n, p, G, Rinv, R, Rtmp, 1, st, gate, nullptr, shift_flag, nullptr));
+    BPF_TRY(tsmm(ctx, n, p, 1, T, 0, Rinv, 0, 1.0, nullptr, 0.0, Q, st, nullptr, gate));
+    // pass 3 (only when a pass needed the shift): Q -> T -> Q
+    BPF_TRY(gram(ctx, n, p, 1, Q, 0, Q, G, 1.0, false, st, gate, nullptr, g3));
+    BPF_TRY(launch_chol(ctx, n, p, G, Rinv, R, Rtmp, 2, st, gate, g3, nullptr, nullptr));
+    BPF_TRY(tsmm(ctx, n, p, 1, Q, 0, Rinv, 0, 1.0, nullptr, 0.0, T, st, nullptr, gate, g3));
+    size_t len = (size_t)n * p;
+    int blocks = std::max(1, std::min(ceil_div((long long)len, 256), ctx->num_sms * 8));
+    gated_copy_kernel<<<blocks, 256, 0, ctx->stream>>>(len, T, Q, st, gate, g3);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+// Psi_i += Phi_i R1 for i < nb; C = C2 R1.  All matrices p x p row-major, R1/C2 upper.
+__global__ void reorth_fold_kernel(int p, int nb, double *__restrict__ Psi,
+                                   const double *__restrict__ Phi, const double *__restrict__ R1,
+                                   const double *__restrict__ C2, double *__restrict__ C,
+                                   double *__restrict__ scratch, const SolveState *st,
+                                   const int *gate) {
+    if (gate_off(st, gate)) return;
+    const size_t pp = (size_t)p * p;
+    const size_t total = (size_t)nb * pp;
+    // blocks 0..nb-1: Psi update; block nb (one extra p x p) : C2 R1 into scratch
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total + pp; e += stride) {
+        if (e < total) {
+            const size_t blk = e / pp;
+            const int a = (int)((e % pp) / p), b = (int)(e % p);
+            const double *ph = Phi + blk * pp + (size_t)a * p;
+            double s = 0.0;
+            for (int c = 0; c <= b; c++) s += ph[c] * R1[(size_t)c * p + b];
+            Psi[e] += s;
+        } else {
+            const size_t f = e - total;
+            const int a = (int)(f / p), b = (int)(f % p);
+            double s = 0.0;
+            for (int c = a; c <= b; c++) s += C2[(size_t)a * p + c] * R1[(size_t)c * p + b];
+            scratch[f] = (b >= a) ? s : 0.0;
+        }
+    }
+}
+
+bpf_status reorth_fold(bpf_ctx *ctx, int p, int nb, double *Psi, const double *Phi,
+                       const double *R1, const double *C2, double *C, double *scratch,
+                       const SolveState *st, const int *gate) {
+    const size_t work = (size_t)(nb + 1) * p * p;
+    int blocks = std::max(1, std::min(ceil_div((long long)work, 256), ctx->num_sms * 4));
+    reorth_fold_kernel<<<blocks, 256, 0, ctx->stream>>>(p, nb, Psi, Phi, R1, C2, C, scratch, st, gate);
+    BPF_LAUNCHED(ctx);
+    const size_t pp = (size_t)p * p;
+    blocks = std::max(1, std::min(ceil_div((long long)pp, 256), ctx->num_sms));
+    gated_copy_kernel<<<blocks, 256, 0, ctx->stream>>>(pp, scratch, C, st, gate, nullptr);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------------------
+// elementwise and reductions
+// ---------------------------------------------------------------------------------------
+__global__ void axpby_kernel(size_t len, double a, const double *__restrict__ x, double b,
+                             double *__restrict__ y, const SolveState *st) {
+    if (st && !st->active) return;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < len;
+         e += (size_t)gridDim.x * blockDim.x)
+        y[e] = a * x[e] + (b == 0.0 ? 0.0 : b * y[e]);
+}
+
+bpf_status axpby(bpf_ctx *ctx, size_t len, double a, const double *x, double b, double *y,
+                 const SolveState *st) {
+    if (len == 0) return BPF_SUCCESS;
+    int blocks = std::max(1, std::min(ceil_div((long long)len, 256), ctx->num_sms * 8));
+    axpby_kernel<<<blocks, 256, 0, ctx->stream>>>(len, a, x, b, y, st);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+// Deterministic two-stage sum of squares: stage 1 one partial per block, stage 2 one block.
+__global__ void sumsq_partial_kernel(size_t len, const double *__restrict__ x,
+                                     double *__restrict__ part) {
+    double s = 0.0;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < len;
+         e += (size_t)gridDim.x * blockDim.x)
+        s += x[e] * x[e];
+    s = warp_sum(s);
+    __shared__ double ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+        v = warp_sum(v);
+        if (threadIdx.x == 0) part[blockIdx.x] = v;
+    }
+}
+
+__global__ void sum_sqrt_kernel(int nparts, const double *__restrict__ part, double *out) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += part[i];
+    s = warp_sum(s);
+    __shared__ double ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+        v = warp_sum(v);
+        if (threadIdx.x == 0) *out = sqrt(v);
+    }
+}
+
+bpf_status frob_norm(bpf_ctx *ctx, size_t len, const double *x, double *out) {
+    bpf_status s;
+    const int nparts = ctx->num_sms * 2;
+    double *buf = (double *)ws_get(ctx, WS_NORM, sizeof(double) * nparts, &s);
+    if (!buf) return s;
+    sumsq_partial_kernel<<<nparts, 256, 0, ctx->stream>>>(len, x, buf);
+    BPF_LAUNCHED(ctx);
+    sum_sqrt_kernel<<<1, 256, 0, ctx->stream>>>(nparts, buf, out);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+}  // namespace bpf
+
+// ---------------------------------------------------------------------------------------
+// C ABI: householder!(Q, R) on a column-major block (src/block_utils.jl:46-53)
+// ---------------------------------------------------------------------------------------
+using namespace bpf;
+
+extern "C" bpf_status bpf_householder(bpf_ctx *ctx, int n, int p, double *Q, int ldq, double *R,
+                                      int ldr) {
+    if (!ctx) return BPF_ERR_INVALID_VALUE;
+    if (n < 0 || p < 0 || (n > 0 && p > 0 && (!Q || !R)))
+        return set_error(ctx, BPF_ERR_INVALID_VALUE, "householder: invalid argument");
+    if (ldq < std::max(1, n) || ldr < std::max(1, p))
+        return set_error(ctx, BPF_ERR_DIMENSION, "householder: leading dimension too small");
+    if (p > n) return set_error(ctx, BPF_ERR_DIMENSION, "householder: n=%d < p=%d", n, p);
+    if (n == 0 || p == 0) return BPF_SUCCESS;
+    if (p > 128) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "householder: p=%d > 128", p);
+    const size_t np = (size_t)n * p, pp = (size_t)p * p;
+    bpf_status s;
+    double *buf = (double *)ws_get(ctx, WS_A, sizeof(double) * (3 * np + 2 * pp), &s);
+    if (!buf) return s;
+    double *W = buf, *Qr = buf + np, *T = buf + 2 * np, *Rr = buf + 3 * np;
+    SolveState *st = (SolveState *)ws_get(ctx, WS_STATE, sizeof(SolveState), &s);
+    if (!st) return s;
+    SolveState hs;
+    memset(&hs, 0, sizeof(hs));
+    hs.active = 1;
+    BPF_CUDA(ctx, cudaMemcpyAsync(st, &hs, sizeof(SolveState), cudaMemcpyHostToDevice, ctx->stream));
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    BPF_TRY(colmajor_to_rowmajor(ctx, n, p, Q, ldq, W));
+    BPF_TRY(cholqr(ctx, n, p, W, Qr, Rr, T, st));
+    BPF_TRY(rowmajor_to_colmajor(ctx, n, p, Qr, Q, ldq));
+    BPF_TRY(rowmajor_to_colmajor(ctx, p, p, Rr, R, ldr));
+    return check_dev_status(ctx, "householder");
+}

@@ -1,0 +1,596 @@
+// block-GMRES: src/block_gmres.jl:127-411 (block_gmres / block_gmres!).
+//
+// The host drives restart passes; the inner Arnoldi iterations run device-resident.  Every
+// kernel of iteration k reads SolveState::active and returns at once when the device-side
+// stopping test (residual <= eps, inner itmax, time limit) has ended the pass, so the host
+// launches a chunk of iterations and synchronises once per chunk instead of once per
+// iteration (the reference syncs on norm(C) every iteration, :342).
+//
+// Per iteration k (k = 1-based, j = k-1):
+//   P = N \ V_j                    one cooperative ILU0/IC0 launch           (:298)
+//   W = A P                        CSR SpMM                                  (:299)
+//   Q = M \ W                      (left preconditioner, if any)             (:300)
+//   Psi = V^T Q, Q -= V Psi  x2    block classical Gram-Schmidt, two passes  (:301-313)
+//   V_{j+1} C = Q                  Cholesky-QR2 (shifted on breakdown)        (:316)
+//   apply Omega_0..Omega_{j-1}     compact-WY block reflectors, p CTAs        (:318-326)
+//   factor [R_jj; C], update Z     one CTA; ||Lambda_{j+1}||_F -> stop test   (:328-353)
+// End of a pass: block back substitution (p CTAs), X += sum V_i Y_i, X <- N X   (:366-385)
+//
+// Numerics vs the reference: two classical Gram-Schmidt passes instead of modified GS
+// (+ optional reorthogonalization), Cholesky-QR instead of Householder for the basis blocks
+// (R has a positive diagonal, LAPACK's may be negative).  Both produce the same Krylov basis
+// up to column signs, so X and the residual history agree up to rounding.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "bpf_internal.cuh"
+#include "dense.cuh"
+#include "prec.cuh"
+
+namespace bpf {
+
+__host__ __device__ inline size_t rpos(int i, int j) { return (size_t)j * (j + 1) / 2 + i; }
+
+__device__ __forceinline__ double block_sum(double v, double *red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        double t = lane < nw ? red[lane] : 0.0;
+        t = warp_sum(t);
+        if (lane == 0) red[0] = t;
+    }
+    __syncthreads();
+    double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// ---------------------------------------------------------------------------------------
+// Apply the stored block reflectors Omega_0..Omega_{j-1} to block column j of the
+// Hessenberg matrix (packed R blocks).  One CTA per column b of the block column; only the
+// two p-segments a reflector touches are held in shared memory.
+// HY layout per block column i: Y_i (2p x p, explicit: 0 above, 1 on the diagonal) then
+// T_i (p x p upper), so Omega_i^T = I - Y_i T_i^T Y_i^T.
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+hess_apply_kernel(int p, int k, double *__restrict__ Rblk, const double *__restrict__ HY,
+                  const SolveState *st) {
+    if (!st->active) return;
+    const int j = k - 1;
+    if (j <= 0) return;
+    const int b = blockIdx.x;
+    extern __shared__ double sm[];
+    double *seg = sm;            // 2p
+    double *w = sm + 2 * p;      // p
+    double *w2 = w + p;          // p
+    const size_t pp = (size_t)p * p;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int a = threadIdx.x; a < p; a += blockDim.x) seg[a] = Rblk[rpos(0, j) * pp + (size_t)a * p + b];
+    for (int i = 0; i < j; i++) {
+        for (int a = threadIdx.x; a < p; a += blockDim.x)
+            seg[p + a] = Rblk[rpos(i + 1, j) * pp + (size_t)a * p + b];
+        __syncthreads();
+        const double *Y = HY + (size_t)i * 3 * pp;
+        const double *T = Y + 2 * pp;
+        for (int c = warp; c < p; c += nw) {
+            double s = 0.0;
+            for (int r = c + lane; r < 2 * p; r += 32) s += Y[(size_t)r * p + c] * seg[r];
+            s = warp_sum(s);
+            if (lane == 0) w[c] = s;
+        }
+        __syncthreads();
+        for (int c = threadIdx.x; c < p; c += blockDim.x) {
+            double s = 0.0;
+            for (int cp = 0; cp <= c; cp++) s += T[(size_t)cp * p + c] * w[cp];
+            w2[c] = s;
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < 2 * p; r += blockDim.x) {
+            const int cmax = min(r, p - 1);
+            double s = 0.0;
+            for (int c = 0; c <= cmax; c++) s += Y[(size_t)r * p + c] * w2[c];
+            seg[r] -= s;
+        }
+        __syncthreads();
+        for (int a = threadIdx.x; a < p; a += blockDim.x) {
+            Rblk[rpos(i, j) * pp + (size_t)a * p + b] = seg[a];
+            seg[a] = seg[p + a];
+        }
+        __syncthreads();
+    }
+    for (int a = threadIdx.x; a < p; a += blockDim.x) Rblk[rpos(j, j) * pp + (size_t)a * p + b] = seg[a];
+}
+
+// ---------------------------------------------------------------------------------------
+// Factor [R_jj; C] (2p x p) with Householder reflections (LAPACK dlarfg conventions), build
+// the compact-WY T factor, apply Omega_j^T to [Z_j; 0], and run the stopping test.
+// One CTA; operands live in global memory (L1-resident), ordered by __syncthreads.
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024)
+hess_factor_kernel(int p, int k, double *__restrict__ Rblk, double *__restrict__ HY,
+                   double *__restrict__ tau_all, double *__restrict__ Z,
+                   const double *__restrict__ Cm, SolveState *st, double *__restrict__ hist,
+                   double *__restrict__ scr) {
+    if (!st->active) return;
+    __shared__ double red[32];
+    __shared__ double s_scale;
+    const int j = k - 1;
+    const size_t pp = (size_t)p * p;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    double *F = HY + (size_t)j * 3 * pp;
+    double *T = F + 2 * pp;
+    double *tau = tau_all;  // reflector scalars of the current block (T keeps them too)
+    double *Rjj = Rblk + rpos(j, j) * pp;
+    double *Zj = Z + (size_t)j * pp;
+    double *Zn = Z + (size_t)(j + 1) * pp;
+    double *YtY = scr, *W1 = scr + pp, *W2 = scr + 2 * pp;
+    const int m = 2 * p;
+    for (size_t e = tid; e < pp; e += nt) {
+        F[e] = Rjj[e];
+        F[pp + e] = Cm[e];
+    }
+    __syncthreads();
+    for (int c = 0; c < p; c++) {
+        double s = 0.0;
+        for (int r = c + 1 + tid; r < m; r += nt) {
+            const double v = F[(size_t)r * p + c];
+            s += v * v;
+        }
+        s = block_sum(s, red);
+        if (tid == 0) {
+            const double alpha = F[(size_t)c * p + c];
+            const double xn = sqrt(s);
+            if (xn == 0.0) {
+                tau[c] = 0.0;
+                s_scale = 0.0;
+            } else {
+                const double beta = -copysign(hypot(alpha, xn), alpha);
+                tau[c] = (beta - alpha) / beta;
+                s_scale = 1.0 / (alpha - beta);
+                F[(size_t)c * p + c] = beta;
+            }
+        }
+        __syncthreads();
+        const double t = tau[c];
+        if (t != 0.0) {
+            const double sc = s_scale;
+            for (int r = c + 1 + tid; r < m; r += nt) F[(size_t)r * p + c] *= sc;
+            __syncthreads();
+            for (int c2 = c + 1 + warp; c2 < p; c2 += nw) {
+                double wv = 0.0;
+                for (int r = c + 1 + lane; r < m; r += 32) wv += F[(size_t)r * p + c] * F[(size_t)r * p + c2];
+                wv = warp_sum(wv) + F[(size_t)c * p + c2];
+                wv *= t;
+                if (lane == 0) F[(size_t)c * p + c2] -= wv;
+                for (int r = c + 1 + lane; r < m; r += 32) F[(size_t)r * p + c2] -= wv * F[(size_t)r * p + c];
+            }
+        }
+        __syncthreads();
+    }
+    // R_jj <- upper triangle; F <- explicit Y
+    for (size_t e = tid; e < pp; e += nt) {
+        const int a = (int)(e / p), b = (int)(e % p);
+        Rjj[e] = (b >= a) ? F[e] : 0.0;
+    }
+    __syncthreads();
+    for (size_t e = tid; e < 2 * pp; e += nt) {
+        const int r = (int)(e / p), c = (int)(e % p);
+        if (r < c) F[e] = 0.0;
+        else if (r == c) F[e] = 1.0;
+    }
+    for (size_t e = tid; e < pp; e += nt) T[e] = 0.0;
+    __syncthreads();
+    // YtY[a][c] = y_a . y_c for a < c (rows r >= c)
+    for (size_t e = tid; e < pp; e += nt) {
+        const int a = (int)(e / p), c = (int)(e % p);
+        if (a < c) {
+            double s = 0.0;
+            for (int r = c; r < m; r++) s += F[(size_t)r * p + a] * F[(size_t)r * p + c];
+            YtY[e] = s;
+        }
+    }
+    __syncthreads();
+    // T(0:c, c) = -tau_c T(0:c, 0:c) YtY(0:c, c); T(c, c) = tau_c   (dlarft, forward)
+    for (int c = 0; c < p; c++) {
+        const double tc = tau[c];
+        for (int a = tid; a < c; a += nt) {
+            double s = 0.0;
+            for (int a2 = a; a2 < c; a2++) s += T[(size_t)a * p + a2] * YtY[(size_t)a2 * p + c];
+            T[(size_t)a * p + c] = -tc * s;
+        }
+        if (tid == 0) T[(size_t)c * p + c] = tc;
+        __syncthreads();
+    }
+    // [Z_j; Lambda] = Omega_j^T [Z_j; 0]
+    for (size_t e = tid; e < pp; e += nt) {
+        const int c = (int)(e / p), b = (int)(e % p);
+        double s = 0.0;
+        for (int r = c; r < p; r++) s += F[(size_t)r * p + c] * Zj[(size_t)r * p + b];
+        W1[e] = s;
+    }
+    __syncthreads();
+    for (size_t e = tid; e < pp; e += nt) {
+        const int c = (int)(e / p), b = (int)(e % p);
+        double s = 0.0;
+        for (int c2 = 0; c2 <= c; c2++) s += T[(size_t)c2 * p + c] * W1[(size_t)c2 * p + b];
+        W2[e] = s;
+    }
+    __syncthreads();
+    double ss = 0.0;
+    for (size_t e = tid; e < 2 * pp; e += nt) {
+        const int r = (int)(e / p), b = (int)(e % p);
+        const int cmax = min(r, p - 1);
+        double s = 0.0;
+        for (int c = 0; c <= cmax; c++) s += F[(size_t)r * p + c] * W2[(size_t)c * p + b];
+        if (r < p) {
+            Zj[e] -= s;
+        } else {
+            Zn[e - pp] = -s;
+            ss += s * s;
+        }
+    }
+    ss = block_sum(ss, red);
+    if (tid == 0) {
+        const double rn = sqrt(ss);
+        st->rnorm = rn;
+        if (st->nres < st->hist_cap) hist[st->nres] = rn;
+        st->nres++;
+        st->inner_iter = k;
+        st->solved = rn <= st->eps;
+        st->inner_tired = st->restart ? (k >= min(st->mem, st->inner_itmax)) : (k >= st->inner_itmax);
+        st->overtimed = (st->deadline_ns != 0ull && globaltimer_ns() > st->deadline_ns);
+        st->active = !(st->solved || st->inner_tired || st->overtimed);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Block back substitution R Y = Z (Y overwrites Z), one CTA per column b of Z (:366-375).
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+backsub_kernel(int p, const double *__restrict__ Rblk, double *__restrict__ Z,
+               const SolveState *st) {
+    const int k = st->inner_iter;
+    const int b = blockIdx.x;
+    extern __shared__ double y[];
+    const size_t pp = (size_t)p * p;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = k - 1; i >= 0; i--) {
+        for (int a = tid; a < p; a += nt) y[a] = Z[(size_t)i * pp + (size_t)a * p + b];
+        __syncthreads();
+        if (warp == 0) {
+            const double *R = Rblk + rpos(i, i) * pp;
+            double v[4];
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const int r = lane + 32 * t;
+                v[t] = r < p ? y[r] : 0.0;
+            }
+            for (int c = p - 1; c >= 0; c--) {
+                const int owner = c & 31, slot = c >> 5;
+                double vc = 0.0;
+#pragma unroll
+                for (int t = 0; t < 4; t++)
+                    if (t == slot) vc = v[t];
+                vc = __shfl_sync(0xffffffffu, vc, owner) / R[(size_t)c * p + c];
+#pragma unroll
+                for (int t = 0; t < 4; t++) {
+                    const int r = lane + 32 * t;
+                    if (r == c) v[t] = vc;
+                    else if (r < c) v[t] -= R[(size_t)r * p + c] * vc;
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const int r = lane + 32 * t;
+                if (r < p) y[r] = v[t];
+            }
+        }
+        __syncthreads();
+        for (int a = tid; a < p; a += nt) Z[(size_t)i * pp + (size_t)a * p + b] = y[a];
+        for (int e = tid; e < i * p; e += nt) {
+            const int i2 = e / p, a = e % p;
+            const double *R = Rblk + rpos(i2, i) * pp + (size_t)a * p;
+            double s = 0.0;
+            for (int c = 0; c < p; c++) s += R[c] * y[c];
+            Z[(size_t)i2 * pp + (size_t)a * p + b] -= s;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void gmres_init_kernel(SolveState *st, double atol, double rtol, double *hist,
+                                  double timemax) {
+    const double r = st->rnorm;
+    st->eps = atol + rtol * r;
+    st->solved = r <= st->eps;
+    if (st->hist_cap > 0) hist[0] = r;
+    st->nres = 1;
+    st->active = 0;
+    st->inner_iter = 0;
+    st->overtimed = 0;
+    st->deadline_ns = (timemax > 0.0 && timemax < 1e15) ? globaltimer_ns() + (unsigned long long)(timemax * 1e9) : 0ull;
+}
+
+__global__ void pass_begin_kernel(SolveState *st, int inner_itmax) {
+    st->inner_itmax = inner_itmax;
+    st->inner_iter = 0;
+    st->inner_tired = 0;
+    st->active = !(st->solved || st->overtimed);
+}
+
+// Grow a workspace slot to `bytes`, keeping its first `keep` bytes.
+bpf_status ws_grow_keep(bpf_ctx *ctx, int slot, size_t bytes, size_t keep) {
+    if (ctx->ws_bytes[slot] >= bytes) return BPF_SUCCESS;
+    void *p = nullptr;
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    BPF_CUDA(ctx, cudaMalloc(&p, bytes));
+    if (ctx->ws[slot] && keep)
+        BPF_CUDA(ctx, cudaMemcpyAsync(p, ctx->ws[slot], std::min(keep, ctx->ws_bytes[slot]),
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->ws[slot]) cudaFree(ctx->ws[slot]);
+    ctx->ws[slot] = p;
+    ctx->ws_bytes[slot] = bytes;
+    return BPF_SUCCESS;
+}
+
+static double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct GmresBufs {
+    double *V, *Rblk, *HY, *tau, *Z;
+    int cap;
+};
+
+static bpf_status gmres_capacity(bpf_ctx *ctx, int n, int p, int cap, int old_cap, GmresBufs &g) {
+    const size_t np = (size_t)n * p, pp = (size_t)p * p;
+    BPF_TRY(ws_grow_keep(ctx, WS_V, sizeof(double) * np * (cap + 1), sizeof(double) * np * (old_cap + 1)));
+    BPF_TRY(ws_grow_keep(ctx, WS_HESS, sizeof(double) * pp * ((size_t)cap * (cap + 1) / 2),
+                         sizeof(double) * pp * ((size_t)old_cap * (old_cap + 1) / 2)));
+    BPF_TRY(ws_grow_keep(ctx, WS_HY, sizeof(double) * (3 * pp + p) * cap,
+                         sizeof(double) * (3 * pp + p) * old_cap));
+    BPF_TRY(ws_grow_keep(ctx, WS_Z, sizeof(double) * pp * (cap + 1), sizeof(double) * pp * (old_cap + 1)));
+    g.V = (double *)ctx->ws[WS_V];
+    g.Rblk = (double *)ctx->ws[WS_HESS];
+    g.HY = (double *)ctx->ws[WS_HY];
+    g.Z = (double *)ctx->ws[WS_Z];
+    g.cap = cap;
+    return BPF_SUCCESS;
+}
+
+}  // namespace bpf
+
+using namespace bpf;
+
+extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p,
+                                      const double *B, int ldb, double *X, int ldx,
+                                      const double *X0, int ldx0, const bpf_prec *M,
+                                      const bpf_prec *N, const bpf_gmres_opts *opts,
+                                      bpf_stats *stats) {
+    if (!ctx) return BPF_ERR_INVALID_VALUE;
+    const double t0 = now_s();
+    if (!A || !opts || !stats) return set_error(ctx, BPF_ERR_INVALID_VALUE, "block_gmres: null argument");
+    const int n = A->n;
+    if (A->dtype != BPF_F64) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "block_gmres: FP64 matrices only");
+    if (n < 1 || p < 1 || !B || !X) return set_error(ctx, BPF_ERR_INVALID_VALUE, "block_gmres: empty system");
+    if (ldb < n || ldx < n || (X0 && ldx0 < n))
+        return set_error(ctx, BPF_ERR_DIMENSION, "Inconsistent problem size");
+    if ((M && M->n != n) || (N && N->n != n))
+        return set_error(ctx, BPF_ERR_DIMENSION, "preconditioner size differs from the system");
+    if ((M || N) && !opts->ldiv)
+        return set_error(ctx, BPF_ERR_NOT_SUPPORTED,
+                         "ILU0/IC0 preconditioners define only ldiv!: pass ldiv=true");
+    if (p > n) return set_error(ctx, BPF_ERR_DIMENSION, "block_gmres: p=%d > n=%d", p, n);
+    if (p > 128) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "block_gmres: p=%d > 128", p);
+    int memory = std::min(n / p, opts->memory);
+    if (memory < 1) memory = 1;
+    const bool restart = opts->restart != 0;
+    int itmax = opts->itmax == 0 ? 2 * (n / p) : opts->itmax;
+    if (itmax < 0) itmax = 0;
+    const double timemax = (opts->timemax > 0.0) ? opts->timemax : 1e300;
+    const size_t np = (size_t)n * p, pp = (size_t)p * p;
+    bpf_status s;
+
+    // n x p working blocks
+    double *vec = (double *)ws_get(ctx, WS_VEC, sizeof(double) * np * 7, &s);
+    if (!vec) return s;
+    double *Bi = vec, *Xi = vec + np, *W = vec + 2 * np, *Qm = vec + 3 * np, *Pm = vec + 4 * np,
+           *dX = vec + 5 * np, *Tq = vec + 6 * np;
+    double *R0 = M ? Qm : W;
+    double *Xr = restart ? dX : Xi;
+    SolveState *st = (SolveState *)ws_get(ctx, WS_STATE, sizeof(SolveState), &s);
+    if (!st) return s;
+    const int hist_cap = itmax + 2;
+    double *hist = (double *)ws_get(ctx, WS_HIST, sizeof(double) * hist_cap, &s);
+    if (!hist) return s;
+    // C (p x p), scratch of the factor kernel (3 p x p), C2 and fold scratch (2 p x p), tau (p)
+    double *Cm = (double *)ws_get(ctx, WS_HSCR, sizeof(double) * (6 * pp + p), &s);
+    if (!Cm) return s;
+    double *scr = Cm + pp;
+    double *C2 = Cm + 4 * pp;
+    double *fold_scr = Cm + 5 * pp;
+    double *tau_cur = Cm + 6 * pp;
+    GmresBufs g{};
+    int cap = restart ? std::min(memory, std::max(itmax, 1)) : std::min(std::max(itmax, 1), std::max(memory, 16));
+    BPF_TRY(gmres_capacity(ctx, n, p, cap, 0, g));
+
+    // State on the host side.
+    SolveState hs;
+    std::memset(&hs, 0, sizeof(hs));
+    hs.itmax = itmax;
+    hs.inner_itmax = itmax;
+    hs.mem = memory;
+    hs.restart = restart;
+    hs.hist_cap = hist_cap;
+    hs.atol = opts->atol;
+    hs.rtol = opts->rtol;
+    BPF_CUDA(ctx, cudaMemcpyAsync(st, &hs, sizeof(SolveState), cudaMemcpyHostToDevice, ctx->stream));
+
+    // Initial residual (:215-227).
+    const int base = A->index_base;
+    const int *rp = A->rowptr, *ci = A->colind;
+    const double *av = (const double *)A->vals;
+    BPF_TRY(colmajor_to_rowmajor(ctx, n, p, B, ldb, Bi));
+    BPF_CUDA(ctx, cudaMemsetAsync(Xi, 0, sizeof(double) * np, ctx->stream));
+    const bool warm = X0 != nullptr;
+    if (warm) {
+        BPF_TRY(colmajor_to_rowmajor(ctx, n, p, X0, ldx0, dX));
+        BPF_TRY(spmm_rowmajor(ctx, n, rp, ci, av, base, p, 1.0, dX, 0.0, W, Bi));
+        if (restart) BPF_CUDA(ctx, cudaMemcpyAsync(Xi, dX, sizeof(double) * np, cudaMemcpyDeviceToDevice, ctx->stream));
+    } else {
+        BPF_CUDA(ctx, cudaMemcpyAsync(W, Bi, sizeof(double) * np, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    if (M) BPF_TRY(prec_apply_rowmajor(ctx, M, p, W, Qm));
+    BPF_TRY(frob_norm(ctx, np, R0, &st->rnorm));
+    gmres_init_kernel<<<1, 1, 0, ctx->stream>>>(st, opts->atol, opts->rtol, hist, timemax - (now_s() - t0));
+    BPF_LAUNCHED(ctx);
+    BPF_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(SolveState), cudaMemcpyDeviceToHost, ctx->stream));
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+
+    if (opts->verbose > 0) {
+        printf("BLOCK-GMRES: system of size %d with %d right-hand sides\n", n, p);
+        printf("%5s  %5s  %7s  %5s\n", "pass", "k", "‖Rₖ‖", "timer");
+        printf("%5d  %5d  %7.1e  %.2fs\n", 0, 0, hs.rnorm, now_s() - t0);
+    }
+    int npass = 0, iter = 0, inner_itmax = itmax;
+    bool solved = hs.solved != 0, tired = iter >= itmax, overtimed = false;
+    int printed = 1;
+    const int chunk = restart ? memory : 16;
+    std::vector<double> hbuf;
+
+    while (!(solved || tired || overtimed)) {
+        pass_begin_kernel<<<1, 1, 0, ctx->stream>>>(st, inner_itmax);
+        BPF_LAUNCHED(ctx);
+        if (restart) {
+            BPF_CUDA(ctx, cudaMemsetAsync(dX, 0, sizeof(double) * np, ctx->stream));
+            if (npass >= 1) {                                               // :267-271
+                BPF_TRY(spmm_rowmajor(ctx, n, rp, ci, av, base, p, 1.0, Xi, 0.0, W, Bi));
+                if (M) BPF_TRY(prec_apply_rowmajor(ctx, M, p, W, Qm));
+            }
+        }
+        BPF_TRY(cholqr(ctx, n, p, R0, g.V, g.Z, Tq, st));                    // :275-276
+        npass++;
+        const int kmax = restart ? std::min(memory, inner_itmax) : inner_itmax;
+        int k = 0;
+        bool active = true;
+        while (active && k < kmax) {
+            const int kend = std::min(kmax, k + chunk);
+            if (kend > g.cap) {
+                int newcap = std::min(std::max(kend, 2 * g.cap), std::max(kmax, 1));
+                BPF_TRY(gmres_capacity(ctx, n, p, newcap, g.cap, g));
+            }
+            // Size the Gram workspaces for the largest k of this chunk up front, so no
+            // allocation (and no implicit synchronisation) happens between launches.
+            double *Psi2buf = (double *)ws_get(ctx, WS_I32, sizeof(double) * pp * kend, &s);
+            if (!Psi2buf) return s;
+            if (!ws_get(ctx, WS_PARTIAL, sizeof(double) * pp * ((size_t)ctx->num_sms * 4 + kend + 1), &s))
+                return s;
+            for (int kk = k + 1; kk <= kend; kk++) {
+                const int jj = kk - 1;
+                double *Vk = g.V + (size_t)jj * np;
+                double *Vn = g.V + (size_t)kk * np;
+                const double *Pk = Vk;
+                if (N) {                                                     // :297-298
+                    BPF_TRY(prec_apply_rowmajor(ctx, N, p, Vk, Pm, &st->active));
+                    Pk = Pm;
+                }
+                BPF_TRY(spmm_rowmajor(ctx, n, rp, ci, av, base, p, 1.0, Pk, 0.0, W, nullptr, &st->active));
+                double *Qk = W;
+                if (M) {                                                     // :300
+                    BPF_TRY(prec_apply_rowmajor(ctx, M, p, W, Qm, &st->active));
+                    Qk = Qm;
+                }
+                double *Psi = g.Rblk + rpos(0, jj) * pp;                     // :301-313
+                BPF_TRY(gram(ctx, n, p, kk, g.V, np, Qk, Psi, 1.0, false, st));
+                BPF_TRY(tsmm(ctx, n, p, kk, g.V, np, Psi, pp, -1.0, Qk, 1.0, Qk, st));
+                BPF_TRY(gram(ctx, n, p, kk, g.V, np, Qk, Psi, 1.0, true, st, nullptr, Psi2buf));
+                BPF_TRY(tsmm(ctx, n, p, kk, g.V, np, Psi2buf, pp, -1.0, Qk, 1.0, Qk, st));
+                BPF_TRY(cholqr(ctx, n, p, Qk, Vn, Cm, Tq, st, nullptr, &st->qr_shift,
+                               &st->qr_reorth));                             // :316
+                // Ill-conditioned block (Cholesky lost > 8 digits): its Q may carry amplified
+                // components along V.  Re-orthogonalize once and fold the correction into the
+                // Hessenberg column: W = V Psi + Q1 R1, Q1 = V Phi + Q2 C2
+                //   => Psi += Phi R1, C = C2 R1.  Gated on the device flag.
+                {
+                    const int *rg = &st->qr_reorth;
+                    BPF_TRY(gram(ctx, n, p, kk, g.V, np, Vn, Psi2buf, 1.0, false, st, rg));
+                    BPF_TRY(tsmm(ctx, n, p, kk, g.V, np, Psi2buf, pp, -1.0, Vn, 1.0, Qk, st, nullptr, rg));
+                    BPF_TRY(cholqr(ctx, n, p, Qk, Vn, C2, Tq, st, rg, &st->qr_shift2, nullptr));
+                    BPF_TRY(reorth_fold(ctx, p, kk, Psi, Psi2buf, Cm, C2, Cm, fold_scr, st, rg));
+                }
+                hess_apply_kernel<<<p, 256, sizeof(double) * 4 * p, ctx->stream>>>(p, kk, g.Rblk, g.HY, st);
+                BPF_LAUNCHED(ctx);
+                hess_factor_kernel<<<1, 1024, 0, ctx->stream>>>(p, kk, g.Rblk, g.HY, tau_cur, g.Z, Cm, st,
+                                                                 hist, scr);
+                BPF_LAUNCHED(ctx);
+            }
+            k = kend;
+            BPF_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(SolveState), cudaMemcpyDeviceToHost, ctx->stream));
+            BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            active = hs.active != 0;
+            if (opts->verbose > 0 && hs.nres > printed) {
+                int upto = std::min(hs.nres, hist_cap);
+                hbuf.resize(upto);
+                BPF_CUDA(ctx, cudaMemcpy(hbuf.data(), hist, sizeof(double) * upto, cudaMemcpyDeviceToHost));
+                for (int q = printed; q < upto; q++) {
+                    const int it = q;  // cumulative iteration index of residual q
+                    if (it % opts->verbose == 0)
+                        printf("%5d  %5d  %7.1e  %.2fs\n", npass, it, hbuf[q], now_s() - t0);
+                }
+                printed = upto;
+            }
+            if (now_s() - t0 > timemax) break;
+        }
+        const int inner_iter = hs.inner_iter;
+        // :366-385
+        backsub_kernel<<<p, 256, sizeof(double) * p, ctx->stream>>>(p, g.Rblk, g.Z, st);
+        BPF_LAUNCHED(ctx);
+        BPF_TRY(tsmm(ctx, n, p, g.cap, g.V, np, g.Z, pp, 1.0, Xr, 1.0, Xr, nullptr, &st->inner_iter));
+        if (N) {
+            BPF_CUDA(ctx, cudaMemcpyAsync(Pm, Xr, sizeof(double) * np, cudaMemcpyDeviceToDevice, ctx->stream));
+            BPF_TRY(prec_apply_rowmajor(ctx, N, p, Pm, Xr));
+        }
+        if (restart) BPF_TRY(axpby(ctx, np, 1.0, dX, 1.0, Xi, nullptr));
+        inner_itmax -= inner_iter;                                          // :388-392
+        iter += inner_iter;
+        tired = iter >= itmax;
+        solved = hs.solved != 0;
+        overtimed = hs.overtimed != 0 || (now_s() - t0 > timemax);
+        if (inner_iter == 0) break;  // nothing progressed (time limit hit before the first iteration)
+    }
+    if (warm && !restart) BPF_TRY(axpby(ctx, np, 1.0, dX, 1.0, Xi, nullptr));   // :402
+    BPF_TRY(rowmajor_to_colmajor(ctx, n, p, Xi, X, ldx));
+    BPF_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(SolveState), cudaMemcpyDeviceToHost, ctx->stream));
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    BPF_TRY(check_dev_status(ctx, "block_gmres"));
+    int status = BPF_SOLVE_UNKNOWN;                                          // :397-399
+    if (tired) status = BPF_SOLVE_ITMAX;
+    if (solved) status = BPF_SOLVE_SOLVED;
+    if (overtimed) status = BPF_SOLVE_TIMEMAX;
+    stats->niter = iter;
+    stats->solved = solved;
+    stats->status = status;
+    stats->npass = npass;
+    stats->n_residuals = opts->history ? std::min(hs.nres, hist_cap) : 0;
+    if (opts->history && stats->residuals && stats->residuals_capacity > 0) {
+        int cnt = std::min(stats->n_residuals, stats->residuals_capacity);
+        BPF_CUDA(ctx, cudaMemcpy(stats->residuals, hist, sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+    }
+    if (opts->verbose > 0) printf("\n");
+    stats->timer = now_s() - t0;
+    return BPF_SUCCESS;
+}

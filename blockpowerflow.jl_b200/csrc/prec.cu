@@ -1,0 +1,496 @@
+// ILU(0) / IC(0) preconditioners: host analysis (level schedules, update lists), device
+// numeric factorization, and the multi-RHS triangular solves of ldiv!.
+//
+// Reference: src/preconditioners_nvidia.jl (ilu0 :42-47 -> csrilu02; ic0 :6-11 -> csric02;
+// ldiv! :13-35, :49-71 -> two cusparseSpSM/SpSV per application).
+//
+// Design (B200):
+//  * One host analysis per sparsity pattern: dependency levels of the forward and backward
+//    solves, rows stored level by level (so a level's rows are contiguous), and for the
+//    numeric factorization the list of (destination, source) update pairs of every L entry.
+//  * The numeric factorization is a cooperative persistent kernel: one warp per row, the
+//    rows of a level spread over the grid, one bounded grid barrier between levels.
+//  * ldiv! is ONE cooperative launch that runs every level of L and then of U (or L'):
+//    a group of G lanes per row, lanes over the p right-hand sides of the row-major block,
+//    the row's (col, val) pairs broadcast by shuffles.  Values written in earlier levels are
+//    read with ld.global.cg (L2, never a stale L1 line).  No scratch vector: the forward
+//    solve writes Y and the backward solve updates Y in place.
+//  * FP32 factors (factor_dtype = BPF_F32) keep float copies of L, U and 1/diag, read half the
+//    factor bytes and compute in FP32; the block stays FP64 in memory.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "bpf_internal.cuh"
+#include "prec.cuh"
+
+namespace bpf {
+
+// ------------------------------------------------------------------------------------
+// host analysis
+// ------------------------------------------------------------------------------------
+// Build a triangular factor from a 0-based CSR pattern.
+//   part 0: strict lower part of each row (forward solve, dependencies c < i)
+//   part 1: strict upper part of each row (backward solve, dependencies c > i)
+//   part 2: transpose of the strict lower part (row i of L' holds L(j,i), j > i)
+// diag[i] (index of A(i,i) in the pattern) gives the diagonal; unit == true ignores it.
+TriHost build_tri(int n, const int *rp, const int *ci, const int *diag, int part, bool unit) {
+    TriHost t;
+    t.n = n;
+    t.unit = unit;
+    // rows of the factor as lists of (col, position-in-pattern)
+    std::vector<int> cnt(n, 0);
+    std::vector<int> frp(n + 1, 0), fci, fpos;
+    if (part == 0 || part == 1) {
+        for (int i = 0; i < n; i++)
+            for (int k = rp[i]; k < rp[i + 1]; k++)
+                if ((part == 0 && ci[k] < i) || (part == 1 && ci[k] > i)) cnt[i]++;
+        for (int i = 0; i < n; i++) frp[i + 1] = frp[i] + cnt[i];
+        fci.resize(frp[n]);
+        fpos.resize(frp[n]);
+        std::vector<int> fill(frp.begin(), frp.end() - 1);
+        for (int i = 0; i < n; i++)
+            for (int k = rp[i]; k < rp[i + 1]; k++)
+                if ((part == 0 && ci[k] < i) || (part == 1 && ci[k] > i)) {
+                    fci[fill[i]] = ci[k];
+                    fpos[fill[i]++] = k;
+                }
+    } else {
+        for (int i = 0; i < n; i++)
+            for (int k = rp[i]; k < rp[i + 1]; k++)
+                if (ci[k] < i) cnt[ci[k]]++;
+        for (int i = 0; i < n; i++) frp[i + 1] = frp[i] + cnt[i];
+        fci.resize(frp[n]);
+        fpos.resize(frp[n]);
+        std::vector<int> fill(frp.begin(), frp.end() - 1);
+        for (int i = 0; i < n; i++)
+            for (int k = rp[i]; k < rp[i + 1]; k++)
+                if (ci[k] < i) {
+                    int r = ci[k];
+                    fci[fill[r]] = i;
+                    fpos[fill[r]++] = k;
+                }
+    }
+    // dependency levels
+    std::vector<int> lev(n, 0);
+    int nlev = 0;
+    if (part == 0) {
+        for (int i = 0; i < n; i++) {
+            int l = 0;
+            for (int k = frp[i]; k < frp[i + 1]; k++) l = std::max(l, lev[fci[k]] + 1);
+            lev[i] = l;
+            nlev = std::max(nlev, l + 1);
+        }
+    } else {
+        for (int i = n - 1; i >= 0; i--) {
+            int l = 0;
+            for (int k = frp[i]; k < frp[i + 1]; k++) l = std::max(l, lev[fci[k]] + 1);
+            lev[i] = l;
+            nlev = std::max(nlev, l + 1);
+        }
+    }
+    if (n == 0) nlev = 0;
+    t.nlev = nlev;
+    t.lev_ptr.assign(nlev + 1, 0);
+    for (int i = 0; i < n; i++) t.lev_ptr[lev[i] + 1]++;
+    for (int l = 0; l < nlev; l++) t.lev_ptr[l + 1] += t.lev_ptr[l];
+    t.rows.resize(n);
+    {
+        std::vector<int> fill(t.lev_ptr.begin(), t.lev_ptr.end() - 1);
+        if (part == 0) {
+            for (int i = 0; i < n; i++) t.rows[fill[lev[i]]++] = i;
+        } else {
+            for (int i = n - 1; i >= 0; i--) t.rows[fill[lev[i]]++] = i;
+        }
+    }
+    t.max_level_rows = 0;
+    for (int l = 0; l < nlev; l++)
+        t.max_level_rows = std::max(t.max_level_rows, t.lev_ptr[l + 1] - t.lev_ptr[l]);
+    // level-sorted row storage
+    t.rp.assign(n + 1, 0);
+    for (int q = 0; q < n; q++) t.rp[q + 1] = t.rp[q] + (frp[t.rows[q] + 1] - frp[t.rows[q]]);
+    t.ci.resize(t.rp[n]);
+    t.map.resize(t.rp[n]);
+    for (int q = 0; q < n; q++) {
+        int i = t.rows[q];
+        std::copy(fci.begin() + frp[i], fci.begin() + frp[i + 1], t.ci.begin() + t.rp[q]);
+        std::copy(fpos.begin() + frp[i], fpos.begin() + frp[i + 1], t.map.begin() + t.rp[q]);
+    }
+    if (!unit) {
+        t.dmap.resize(n);
+        for (int q = 0; q < n; q++) t.dmap[q] = diag[t.rows[q]];
+    }
+    return t;
+}
+
+// ILU(0) update pairs: for the L entry e = (i,k), every j > k with (k,j) and (i,j) both in
+// the pattern gives (dst = pos(i,j), src = pos(k,j)); applied as fv[dst] -= fv[e] * fv[src].
+// IC(0) pairs: for the L entry e = (i,k), every j < k with (i,j) and (k,j) in the lower
+// pattern gives (pos(i,j), pos(k,j)); fv[e] -= sum fv[pos(i,j)] * fv[pos(k,j)].
+void build_pairs(int n, const int *rp, const int *ci, const int *diag, bool ic,
+                 std::vector<int> &pp, std::vector<int> &pdst, std::vector<int> &psrc) {
+    int nnz = rp[n];
+    pp.assign(nnz + 1, 0);
+    pdst.clear();
+    psrc.clear();
+    std::vector<int> pos(n, -1);
+    for (int i = 0; i < n; i++) {
+        for (int k = rp[i]; k < rp[i + 1]; k++) pos[ci[k]] = k;
+        for (int e = rp[i]; e < rp[i + 1]; e++) {
+            pp[e] = (int)pdst.size();
+            int kc = ci[e];
+            if (kc >= i) continue;
+            if (!ic) {
+                for (int j = diag[kc] + 1; j < rp[kc + 1]; j++) {
+                    int q = pos[ci[j]];
+                    if (q >= 0) {
+                        pdst.push_back(q);
+                        psrc.push_back(j);
+                    }
+                }
+            } else {
+                for (int j = rp[kc]; j < diag[kc]; j++) {
+                    int q = pos[ci[j]];
+                    if (q >= 0 && ci[j] < kc) {
+                        pdst.push_back(q);
+                        psrc.push_back(j);
+                    }
+                }
+            }
+        }
+        for (int k = rp[i]; k < rp[i + 1]; k++) pos[ci[k]] = -1;
+    }
+    pp[nnz] = (int)pdst.size();
+}
+
+// ------------------------------------------------------------------------------------
+// device helpers for the TriDev struct
+// ------------------------------------------------------------------------------------
+template <typename T>
+static bpf_status upload(bpf_ctx *ctx, T **dptr, const std::vector<T> &h) {
+    *dptr = nullptr;
+    if (h.empty()) return BPF_SUCCESS;
+    BPF_CUDA(ctx, cudaMalloc((void **)dptr, sizeof(T) * h.size()));
+    BPF_CUDA(ctx, cudaMemcpyAsync(*dptr, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    return BPF_SUCCESS;
+}
+
+bpf_status tri_upload(bpf_ctx *ctx, const TriHost &h, TriDev &d) {
+    d.n = h.n;
+    d.nlev = h.nlev;
+    d.nnz = (int)h.ci.size();
+    d.unit = h.unit;
+    d.max_level_rows = h.max_level_rows;
+    d.lev_ptr_h = h.lev_ptr;
+    BPF_TRY(upload(ctx, &d.lev_ptr, h.lev_ptr));
+    BPF_TRY(upload(ctx, &d.rows, h.rows));
+    BPF_TRY(upload(ctx, &d.rp, h.rp));
+    BPF_TRY(upload(ctx, &d.ci, h.ci));
+    BPF_TRY(upload(ctx, &d.map, h.map));
+    BPF_TRY(upload(ctx, &d.dmap, h.dmap));
+    if (d.nnz > 0) {
+        BPF_CUDA(ctx, cudaMalloc((void **)&d.val, sizeof(double) * d.nnz));
+        BPF_CUDA(ctx, cudaMalloc((void **)&d.valf, sizeof(float) * d.nnz));
+    }
+    if (!h.unit && h.n > 0) {
+        BPF_CUDA(ctx, cudaMalloc((void **)&d.dinv, sizeof(double) * h.n));
+        BPF_CUDA(ctx, cudaMalloc((void **)&d.dinvf, sizeof(float) * h.n));
+    }
+    return BPF_SUCCESS;
+}
+
+void tri_free(TriDev &d) {
+    cudaFree(d.lev_ptr);
+    cudaFree(d.rows);
+    cudaFree(d.rp);
+    cudaFree(d.ci);
+    cudaFree(d.map);
+    cudaFree(d.dmap);
+    cudaFree(d.val);
+    cudaFree(d.valf);
+    cudaFree(d.dinv);
+    cudaFree(d.dinvf);
+    d = TriDev();
+}
+
+// Copy factor values (pattern order) into the level-sorted triangular storage.
+__global__ void tri_scatter_kernel(TriKernelArgs t, const double *__restrict__ fv) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < t.nnz; e += stride) {
+        double v = fv[t.map[e]];
+        t.val[e] = v;
+        t.valf[e] = (float)v;
+    }
+    if (t.dinv) {
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < t.n; q += stride) {
+            double d = 1.0 / fv[t.dmap[q]];
+            t.dinv[q] = d;
+            t.dinvf[q] = (float)d;
+        }
+    }
+}
+
+bpf_status tri_scatter(bpf_ctx *ctx, const TriDev &d, const double *fv) {
+    if (d.n == 0) return BPF_SUCCESS;
+    int work = std::max(d.nnz, d.n);
+    int blocks = std::min(ceil_div(work, 256), ctx->num_sms * 8);
+    tri_scatter_kernel<<<blocks, 256, 0, ctx->stream>>>(d.args(), fv);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+// ------------------------------------------------------------------------------------
+// numeric factorization (cooperative, level by level, one warp per row)
+// ------------------------------------------------------------------------------------
+struct FactorArgs {
+    int n;
+    const int *rp;      // pattern (0-based)
+    const int *ci;
+    const int *diag;
+    const int *pp;      // pair pointer per pattern entry (nnz+1)
+    const int *pdst;
+    const int *psrc;
+    const int *lev_ptr; // level schedule of the forward dependencies
+    const int *rows;
+    int nlev;
+    int ic;             // 0 ILU0, 1 IC0
+    double *fv;         // factor values (pattern order), in/out
+    DevStatus *ds;
+};
+
+__global__ void __launch_bounds__(256) factor_coop_kernel(FactorArgs a) {
+    __shared__ unsigned s_gen;
+    if (threadIdx.x == 0) s_gen = barrier_gen_start(a.ds);
+    __syncthreads();
+    unsigned gen = s_gen;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    const int gw = blockIdx.x * wpb + (threadIdx.x >> 5);
+    const int nw = gridDim.x * wpb;
+    double *fv = a.fv;
+    for (int l = 0; l < a.nlev; l++) {
+        const int q0 = a.lev_ptr[l], q1 = a.lev_ptr[l + 1];
+        for (int q = q0 + gw; q < q1; q += nw) {
+            const int i = a.rows[q];
+            const int rs = a.rp[i], di = a.diag[i];
+            for (int e = rs; e < di; e++) {
+                const int k = a.ci[e];
+                const int p0 = a.pp[e], p1 = a.pp[e + 1];
+                if (!a.ic) {
+                    double l_ik = 0.0;
+                    if (lane == 0) {
+                        const double piv = __ldcg(fv + a.diag[k]);
+                        l_ik = __ldcg(fv + e) / piv;
+                        fv[e] = l_ik;
+                        if (piv == 0.0) {
+                            if (atomicCAS(&a.ds->err, 0, (int)DEV_ZERO_PIVOT) == 0) a.ds->aux = k;
+                        }
+                    }
+                    l_ik = __shfl_sync(0xffffffffu, l_ik, 0);
+                    for (int t = p0 + lane; t < p1; t += 32) {
+                        const int d = a.pdst[t];
+                        fv[d] = __ldcg(fv + d) - l_ik * __ldcg(fv + a.psrc[t]);
+                    }
+                } else {
+                    double s = 0.0;
+                    for (int t = p0 + lane; t < p1; t += 32)
+                        s += __ldcg(fv + a.pdst[t]) * __ldcg(fv + a.psrc[t]);
+                    s = warp_sum(s);
+                    if (lane == 0) fv[e] = (__ldcg(fv + e) - s) / __ldcg(fv + a.diag[k]);
+                }
+                __syncwarp();
+            }
+            if (a.ic) {
+                double s = 0.0;
+                for (int e = rs + lane; e < di; e += 32) {
+                    double v = __ldcg(fv + e);
+                    s += v * v;
+                }
+                s = warp_sum(s);
+                if (lane == 0) {
+                    double d = __ldcg(fv + di) - s;
+                    if (!(d > 0.0)) {
+                        if (atomicCAS(&a.ds->err, 0, (int)DEV_ZERO_PIVOT) == 0) a.ds->aux = i;
+                        d = 1.0;
+                    }
+                    fv[di] = sqrt(d);
+                }
+            } else if (lane == 0) {
+                if (__ldcg(fv + di) == 0.0) {
+                    if (atomicCAS(&a.ds->err, 0, (int)DEV_ZERO_PIVOT) == 0) a.ds->aux = i;
+                }
+            }
+            __syncwarp();
+        }
+        if (l + 1 < a.nlev) {
+            if (!grid_barrier(a.ds, gen)) return;
+        }
+    }
+}
+
+// Cooperative grid size: enough blocks for the widest level, capped by co-residency.
+template <typename K>
+static bpf_status coop_grid(bpf_ctx *ctx, K kernel, int threads, size_t smem, int want,
+                            int *grid) {
+    int per_sm = 0;
+    BPF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+    if (per_sm < 1) return set_error(ctx, BPF_ERR_CUDA, "cooperative kernel does not fit on an SM");
+    int cap = per_sm * ctx->num_sms;
+    *grid = std::max(1, std::min(want, cap));
+    return BPF_SUCCESS;
+}
+
+bpf_status factor_numeric(bpf_ctx *ctx, bpf_prec *P) {
+    FactorArgs a;
+    a.n = P->n;
+    a.rp = P->rp;
+    a.ci = P->ci;
+    a.diag = P->diag;
+    a.pp = P->pp;
+    a.pdst = P->pdst;
+    a.psrc = P->psrc;
+    a.lev_ptr = P->lower.lev_ptr;
+    a.rows = P->lower.rows;
+    a.nlev = P->lower.nlev;
+    a.ic = P->kind == PREC_IC0;
+    a.fv = P->fv;
+    a.ds = ctx->dstat;
+    if (P->n == 0) return BPF_SUCCESS;
+    int want = ceil_div(P->lower.max_level_rows, 8);
+    int grid = 1;
+    BPF_TRY(coop_grid(ctx, factor_coop_kernel, 256, 0, want, &grid));
+    void *args[] = {&a};
+    BPF_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)factor_coop_kernel, dim3(grid),
+                                              dim3(256), args, 0, ctx->stream));
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+// ------------------------------------------------------------------------------------
+// triangular solves (cooperative; all levels of both factors in one launch)
+// ------------------------------------------------------------------------------------
+template <int G, int CPL, typename TF, bool IN_F32, bool OUT_F32>
+__global__ void __launch_bounds__(512)
+trsv2_coop_kernel(TriKernelArgs t0, TriKernelArgs t1, int p, const void *Xv, void *Yv,
+                  DevStatus *ds, const int *gate) {
+    if (gate && *gate == 0) return;
+    __shared__ unsigned s_gen;
+    if (threadIdx.x == 0) s_gen = barrier_gen_start(ds);
+    __syncthreads();
+    unsigned gen = s_gen;
+    using TIn = typename std::conditional<IN_F32, float, double>::type;
+    using TOut = typename std::conditional<OUT_F32, float, double>::type;
+    const TIn *X = (const TIn *)Xv;
+    TOut *Y = (TOut *)Yv;
+    const int lane = threadIdx.x & 31;
+    const int glane = lane % G;
+    const int gpb = blockDim.x / G;
+    const int gid = blockIdx.x * gpb + threadIdx.x / G;
+    const int ng = gridDim.x * gpb;
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane / G * G));
+#pragma unroll 1
+    for (int phase = 0; phase < 2; phase++) {
+        const TriKernelArgs &t = phase == 0 ? t0 : t1;
+        const TF *val = std::is_same<TF, float>::value ? (const TF *)t.valf : (const TF *)t.val;
+        const TF *dinv = std::is_same<TF, float>::value ? (const TF *)t.dinvf : (const TF *)t.dinv;
+        for (int l = 0; l < t.nlev; l++) {
+            const int q0 = __ldg(t.lev_ptr + l), q1 = __ldg(t.lev_ptr + l + 1);
+            for (int q = q0 + gid; q < q1; q += ng) {
+                const int i = __ldg(t.rows + q);
+                TF acc[CPL];
+#pragma unroll
+                for (int j = 0; j < CPL; j++) {
+                    const int col = glane + j * G;
+                    if (col < p) {
+                        if (phase == 0) acc[j] = (TF)X[(size_t)i * p + col];
+                        else acc[j] = (TF)__ldcg(Y + (size_t)i * p + col);
+                    } else {
+                        acc[j] = (TF)0;
+                    }
+                }
+                const int rs = __ldg(t.rp + q), re = __ldg(t.rp + q + 1);
+                for (int kb = rs; kb < re; kb += G) {
+                    const int k = kb + glane;
+                    int c = 0;
+                    TF a = (TF)0;
+                    if (k < re) {
+                        c = __ldg(t.ci + k);
+                        a = __ldg(val + k);
+                    }
+                    const int cnt = min(G, re - kb);
+                    for (int s = 0; s < cnt; s++) {
+                        const int cs = __shfl_sync(gmask, c, s, G);
+                        const TF as = __shfl_sync(gmask, a, s, G);
+                        const TOut *yr = Y + (size_t)cs * p;
+#pragma unroll
+                        for (int j = 0; j < CPL; j++) {
+                            const int col = glane + j * G;
+                            if (col < p) acc[j] -= as * (TF)__ldcg(yr + col);
+                        }
+                    }
+                }
+                TF dv = (TF)1;
+                if (dinv) dv = __ldg(dinv + q);
+                TOut *yi = Y + (size_t)i * p;
+#pragma unroll
+                for (int j = 0; j < CPL; j++) {
+                    const int col = glane + j * G;
+                    if (col < p) yi[col] = (TOut)(acc[j] * dv);
+                }
+            }
+            const bool last = (phase == 1 && l + 1 == t.nlev);
+            if (!last) {
+                if (!grid_barrier(ds, gen)) return;
+            }
+        }
+    }
+}
+
+template <int G, int CPL, typename TF, bool IN_F32, bool OUT_F32>
+static bpf_status launch_trsv2(bpf_ctx *ctx, const TriDev &t0, const TriDev &t1, int p,
+                               const void *X, void *Y, const int *gate) {
+    auto kern = trsv2_coop_kernel<G, CPL, TF, IN_F32, OUT_F32>;
+    const int maxrows = std::max(t0.max_level_rows, t1.max_level_rows);
+    int threads, grid;
+    // Small levels: one block of 512 threads, barriers are __syncthreads.
+    if (maxrows <= 2 * (512 / G)) {
+        threads = 512;
+        grid = 1;
+    } else {
+        threads = 256;
+        BPF_TRY(coop_grid(ctx, kern, threads, 0, ceil_div(maxrows, threads / G), &grid));
+    }
+    TriKernelArgs a0 = t0.args(), a1 = t1.args();
+    DevStatus *ds = ctx->dstat;
+    void *args[] = {&a0, &a1, &p, (void *)&X, &Y, &ds, (void *)&gate};
+    BPF_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)kern, dim3(grid), dim3(threads), args, 0,
+                                              ctx->stream));
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+template <typename TF, bool IN_F32, bool OUT_F32>
+static bpf_status trsv2_dispatch(bpf_ctx *ctx, const TriDev &t0, const TriDev &t1, int p,
+                                 const void *X, void *Y, const int *gate) {
+    if (p <= 4) return launch_trsv2<4, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
+    if (p <= 8) return launch_trsv2<8, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
+    if (p <= 16) return launch_trsv2<16, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
+    if (p <= 32) return launch_trsv2<32, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
+    if (p <= 64) return launch_trsv2<32, 2, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
+    if (p <= 128) return launch_trsv2<32, 4, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
+    if (p <= 256) return launch_trsv2<32, 8, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
+    return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "triangular solve: p=%d > 256 per call", p);
+}
+
+// Y = P \ X on row-major n x p blocks (FP64 in/out).  Blocks wider than 256 columns are
+// solved in 256-column slices by the caller.
+bpf_status prec_apply_rowmajor(bpf_ctx *ctx, const bpf_prec *P, int p, const double *X,
+                               double *Y, const int *gate) {
+    if (P->n == 0 || p == 0) return BPF_SUCCESS;
+    if (P->fdtype == BPF_F32)
+        return trsv2_dispatch<float, false, false>(ctx, P->lower, P->upper, p, X, Y, gate);
+    return trsv2_dispatch<double, false, false>(ctx, P->lower, P->upper, p, X, Y, gate);
+}
+
+}  // namespace bpf

@@ -1,0 +1,98 @@
+// Internal types of the preconditioner / triangular-factor machinery.
+#pragma once
+
+#include <type_traits>
+#include <vector>
+
+#include "bpf_internal.cuh"
+
+namespace bpf {
+
+// A triangular factor analysed on the host: rows stored level by level.
+struct TriHost {
+    int n = 0;
+    int nlev = 0;
+    int max_level_rows = 0;
+    bool unit = true;
+    std::vector<int> lev_ptr;  // nlev+1, positions into rows
+    std::vector<int> rows;     // n, row id at each level-sorted position
+    std::vector<int> rp;       // n+1, per level-sorted position
+    std::vector<int> ci;       // off-diagonal column ids
+    std::vector<int> map;      // position of each off-diagonal entry in the source pattern
+    std::vector<int> dmap;     // position of the diagonal in the source pattern (non-unit)
+};
+
+// Plain-pointer view passed to kernels.
+struct TriKernelArgs {
+    int n, nlev, nnz;
+    const int *lev_ptr, *rows, *rp, *ci, *map, *dmap;
+    double *val;
+    float *valf;
+    double *dinv;
+    float *dinvf;
+};
+
+struct TriDev {
+    int n = 0, nlev = 0, nnz = 0, max_level_rows = 0;
+    bool unit = true;
+    std::vector<int> lev_ptr_h;
+    int *lev_ptr = nullptr, *rows = nullptr, *rp = nullptr, *ci = nullptr, *map = nullptr,
+        *dmap = nullptr;
+    double *val = nullptr;
+    float *valf = nullptr;
+    double *dinv = nullptr;
+    float *dinvf = nullptr;
+    TriKernelArgs args() const {
+        TriKernelArgs a;
+        a.n = n;
+        a.nlev = nlev;
+        a.nnz = nnz;
+        a.lev_ptr = lev_ptr;
+        a.rows = rows;
+        a.rp = rp;
+        a.ci = ci;
+        a.map = map;
+        a.dmap = dmap;
+        a.val = val;
+        a.valf = valf;
+        a.dinv = dinv;
+        a.dinvf = dinvf;
+        return a;
+    }
+};
+
+enum PrecKind { PREC_ILU0 = 1, PREC_IC0 = 2, PREC_LU = 3 };
+
+TriHost build_tri(int n, const int *rp, const int *ci, const int *diag, int part, bool unit);
+void build_pairs(int n, const int *rp, const int *ci, const int *diag, bool ic,
+                 std::vector<int> &pp, std::vector<int> &pdst, std::vector<int> &psrc);
+bpf_status tri_upload(bpf_ctx *ctx, const TriHost &h, TriDev &d);
+void tri_free(TriDev &d);
+bpf_status tri_scatter(bpf_ctx *ctx, const TriDev &d, const double *fv);
+
+}  // namespace bpf
+
+// The preconditioner object behind the C ABI (NVIDIA_ILU0 / NVIDIA_IC0).
+struct bpf_prec {
+    bpf_ctx *ctx = nullptr;
+    int kind = 0;
+    int n = 0, nnz = 0, nrhs = 0;
+    int fdtype = BPF_F64;
+    // pattern (0-based device copies) and factor values in pattern order
+    int *rp = nullptr, *ci = nullptr, *diag = nullptr;
+    double *fv = nullptr;
+    int *pp = nullptr, *pdst = nullptr, *psrc = nullptr;
+    long long npairs = 0;
+    bpf::TriDev lower;   // forward solve (L unit for ILU0; L for IC0)
+    bpf::TriDev upper;   // backward solve (U for ILU0; L' for IC0)
+};
+
+namespace bpf {
+bpf_status prec_setup(bpf_ctx *ctx, int kind, int n, const std::vector<int> &rp,
+                      const std::vector<int> &ci, const std::vector<int> &diag, bpf_prec **out);
+bpf_status csr_pattern_to_host(bpf_ctx *ctx, const bpf_csr_desc *A, std::vector<int> &rp,
+                               std::vector<int> &ci, bool need_diag, std::vector<int> *diag);
+bpf_status factor_numeric(bpf_ctx *ctx, bpf_prec *P);
+bpf_status prec_apply_rowmajor(bpf_ctx *ctx, const bpf_prec *P, int p, const double *X,
+                               double *Y, const int *gate = nullptr);
+}  // namespace bpf

@@ -1,0 +1,170 @@
+// CSR SpMM on row-major (RHS-interleaved) blocks, and the column-major <-> row-major
+// conversions at the API boundary.
+//
+// Replaces mul!(W, A, P) (src/block_gmres.jl:299, :220,268; src/block_bicgstab.jl:135,145,
+// 252,264), which CUDA.jl maps to cusparseSpMM on column-major blocks.  Here the block is
+// stored row-major (the p values of one unknown are contiguous), so every nonzero a_ij
+// gathers one contiguous p-vector of X: a group of G lanes per row reads it with coalesced
+// loads while the row's (col, val) pairs are loaded once per group and broadcast by shuffles.
+//
+// Algorithmic bytes per launch: 12*nnz + 4*(n+1) + 8*n*p (X) + 8*n*p (Y written)
+// [+ 8*n*p when beta != 0 or the residual form reads B].
+#include "bpf_internal.cuh"
+
+namespace bpf {
+
+template <int G, int CPL, typename TX>
+__global__ void __launch_bounds__(256)
+spmm_rm_kernel(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+               const double *__restrict__ av, int base, int p, double alpha,
+               const TX *__restrict__ X, double beta, double *__restrict__ Y,
+               const double *__restrict__ Bres, const int *gate) {
+    if (gate && *gate == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int glane = lane % G;                    // lane within the row group
+    const int groups_per_block = blockDim.x / G;
+    const int grp = blockIdx.x * groups_per_block + threadIdx.x / G;
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane / G * G));
+    for (int row = grp; row < n; row += gridDim.x * groups_per_block) {
+        double acc[CPL];
+#pragma unroll
+        for (int j = 0; j < CPL; j++) acc[j] = 0.0;
+        const int rs = __ldg(rp + row) - base, re = __ldg(rp + row + 1) - base;
+        for (int kb = rs; kb < re; kb += G) {
+            int k = kb + glane;
+            int c = 0;
+            double a = 0.0;
+            if (k < re) {
+                c = __ldg(ci + k) - base;
+                a = __ldg(av + k);
+            }
+            const int cnt = min(G, re - kb);
+            for (int t = 0; t < cnt; t++) {
+                const int ct = __shfl_sync(gmask, c, t, G);
+                const double at = __shfl_sync(gmask, a, t, G);
+                const TX *xr = X + (size_t)ct * p;
+#pragma unroll
+                for (int j = 0; j < CPL; j++) {
+                    const int col = glane + j * G;
+                    if (col < p) acc[j] += at * (double)__ldg(xr + col);
+                }
+            }
+        }
+        double *yr = Y + (size_t)row * p;
+#pragma unroll
+        for (int j = 0; j < CPL; j++) {
+            const int col = glane + j * G;
+            if (col < p) {
+                double v;
+                if (Bres) {
+                    v = Bres[(size_t)row * p + col] - acc[j];
+                } else {
+                    v = alpha * acc[j];
+                    if (beta != 0.0) v += beta * yr[col];
+                }
+                yr[col] = v;
+            }
+        }
+    }
+}
+
+template <int G, int CPL, typename TX>
+static bpf_status launch_spmm(bpf_ctx *ctx, int n, const int *rp, const int *ci,
+                              const double *av, int base, int p, double alpha, const TX *X,
+                              double beta, double *Y, const double *B, const int *gate) {
+    const int threads = 256;
+    const int groups = threads / G;
+    long long blocks_needed = ceil_div(n, groups);
+    int blocks = (int)std::min<long long>(blocks_needed, (long long)ctx->num_sms * 16);
+    if (blocks < 1) blocks = 1;
+    spmm_rm_kernel<G, CPL, TX><<<blocks, threads, 0, ctx->stream>>>(n, rp, ci, av, base, p, alpha,
+                                                                    X, beta, Y, B, gate);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+template <typename TX>
+static bpf_status spmm_dispatch(bpf_ctx *ctx, int n, const int *rp, const int *ci,
+                                const double *av, int base, int p, double alpha, const TX *X,
+                                double beta, double *Y, const double *B, const int *gate) {
+    if (n == 0 || p == 0) return BPF_SUCCESS;
+    if (p <= 4) return launch_spmm<4, 1>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    if (p <= 8) return launch_spmm<8, 1>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    if (p <= 16) return launch_spmm<16, 1>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    if (p <= 32) return launch_spmm<32, 1>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    if (p <= 64) return launch_spmm<32, 2>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    if (p <= 128) return launch_spmm<32, 4>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    if (p <= 256) return launch_spmm<32, 8>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    return launch_spmm<32, 16>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+}
+
+bpf_status spmm_rowmajor(bpf_ctx *ctx, int n, const int *rp, const int *ci, const double *av,
+                         int base, int p, double alpha, const double *X, double beta,
+                         double *Y, const double *B, const int *gate) {
+    if (p > 512) {
+        return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "spmm: p=%d > 512 right-hand sides", p);
+    }
+    return spmm_dispatch<double>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+}
+
+bpf_status spmm_rowmajor_f32x(bpf_ctx *ctx, int n, const int *rp, const int *ci,
+                              const double *av, int base, int p, const float *X, double *Y,
+                              const int *gate) {
+    if (p > 512) {
+        return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "spmm: p=%d > 512 right-hand sides", p);
+    }
+    return spmm_dispatch<float>(ctx, n, rp, ci, av, base, p, 1.0, X, 0.0, Y, nullptr, gate);
+}
+
+// ------------------------------------------------------------------------------------
+// layout conversions (32x32 tiles through shared memory)
+// ------------------------------------------------------------------------------------
+__global__ void cm_to_rm_kernel(int n, int p, const double *__restrict__ src, int ld,
+                                double *__restrict__ dst) {
+    __shared__ double tile[32][33];
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int c = c0 + j, r = r0 + threadIdx.x;
+        if (r < n && c < p) tile[j][threadIdx.x] = src[(size_t)c * ld + r];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int r = r0 + j, c = c0 + threadIdx.x;
+        if (r < n && c < p) dst[(size_t)r * p + c] = tile[threadIdx.x][j];
+    }
+}
+
+__global__ void rm_to_cm_kernel(int n, int p, const double *__restrict__ src,
+                                double *__restrict__ dst, int ld) {
+    __shared__ double tile[32][33];
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int r = r0 + j, c = c0 + threadIdx.x;
+        if (r < n && c < p) tile[j][threadIdx.x] = src[(size_t)r * p + c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int c = c0 + j, r = r0 + threadIdx.x;
+        if (r < n && c < p) dst[(size_t)c * ld + r] = tile[threadIdx.x][j];
+    }
+}
+
+bpf_status colmajor_to_rowmajor(bpf_ctx *ctx, int n, int p, const double *src, int ld,
+                                double *dst) {
+    if (n == 0 || p == 0) return BPF_SUCCESS;
+    dim3 grid(ceil_div(n, 32), ceil_div(p, 32)), block(32, 8);
+    cm_to_rm_kernel<<<grid, block, 0, ctx->stream>>>(n, p, src, ld, dst);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+bpf_status rowmajor_to_colmajor(bpf_ctx *ctx, int n, int p, const double *src, double *dst,
+                                int ld) {
+    if (n == 0 || p == 0) return BPF_SUCCESS;
+    dim3 grid(ceil_div(n, 32), ceil_div(p, 32)), block(32, 8);
+    rm_to_cm_kernel<<<grid, block, 0, ctx->stream>>>(n, p, src, dst, ld);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+}  // namespace bpf

@@ -1,0 +1,210 @@
+/*
+ * bpf.h -- C ABI of libbpf.so, the B200 (sm_100a) multi-RHS sparse solve library.
+ *
+ * Each entry point replaces one call of exanauts/BlockPowerFlow.jl (Julia) that a host
+ * binding (ccall from Julia, ctypes from Python) forwards here.  The reference interface each
+ * one stands in for is cited beside it as `file:line` of that project.
+ *
+ * Conventions
+ *  - Every function returns a bpf_status; on failure bpf_last_error(ctx) says why.
+ *  - Dense blocks (B, X, Y, ...) are DEVICE pointers to column-major n x p matrices with an
+ *    explicit leading dimension (Julia's CuMatrix{Float64}).  Internal layouts are private.
+ *  - CSR descriptors hold DEVICE pointers and are borrowed: the library never frees them.
+ *    index_base 1 accepts CUDA.jl's 1-based CuSparseMatrixCSR arrays as they are.
+ *  - All work is ordered on the context's stream.  A call returns only after the stream has
+ *    finished when it has to hand host scalars back (solver statistics); the others are
+ *    asynchronous with respect to the host.
+ *  - A context is not thread-safe: use one per host thread / Julia task.
+ */
+#ifndef BPF_H_
+#define BPF_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define BPF_API __attribute__((visibility("default")))
+#else
+#define BPF_API
+#endif
+
+typedef enum {
+    BPF_SUCCESS = 0,
+    BPF_ERR_INVALID_VALUE = 1,  /* bad argument (null pointer, negative size, ...)        */
+    BPF_ERR_DIMENSION = 2,      /* "System must be square" / "Inconsistent problem size" */
+    BPF_ERR_CUDA = 3,           /* a CUDA runtime call failed                            */
+    BPF_ERR_ALLOC = 4,          /* device or host allocation failed                      */
+    BPF_ERR_SINGULAR = 5,       /* zero / non-positive pivot in a factorization           */
+    BPF_ERR_NOT_SUPPORTED = 6,  /* option combination the reference rejects as well      */
+    BPF_ERR_TIMEOUT = 7,        /* a bounded device-side wait gave up                    */
+    BPF_ERR_NUMERIC = 8         /* NaN/Inf met where the algorithm cannot continue       */
+} bpf_status;
+
+typedef enum { BPF_F64 = 0, BPF_F32 = 1 } bpf_dtype;
+
+/* Termination status of a Krylov solve; bpf_solve_status_string gives the reference's text
+ * (src/block_gmres.jl:397-399, src/block_bicgstab.jl:160-171). */
+typedef enum {
+    BPF_SOLVE_UNKNOWN = 0,
+    BPF_SOLVE_SOLVED = 1,       /* "solution good enough given atol and rtol" */
+    BPF_SOLVE_ITMAX = 2,        /* "maximum number of iterations exceeded"    */
+    BPF_SOLVE_TIMEMAX = 3       /* "time limit exceeded"                      */
+} bpf_solve_status;
+
+/* Fill-reducing orderings of the RF analysis (src/cusolverRF.jl:70-95). */
+typedef enum {
+    BPF_ORDER_AMD = 0,      /* :AMD   (reference default)                          */
+    BPF_ORDER_MDQ = 1,      /* :MDQ   minimum degree on the quotient graph          */
+    BPF_ORDER_METIS = 2,    /* :METIS nested dissection                             */
+    BPF_ORDER_RCM = 3,      /* :RCM   reverse Cuthill-McKee                          */
+    BPF_ORDER_NATURAL = 4   /* no reordering                                         */
+} bpf_ordering;
+
+/* Arithmetic of the preconditioner's triangular factors.  BPF_F32 keeps an FP32 copy of the
+ * factors and runs the triangular solves in FP32 (FP64 in / FP64 out). */
+typedef bpf_dtype bpf_factor_dtype;
+
+typedef struct bpf_ctx bpf_ctx;
+typedef struct bpf_prec bpf_prec;
+typedef struct bpf_rf bpf_rf;
+
+/* CuSparseMatrixCSR{Float64,Cint}: n x n, device arrays, borrowed. */
+typedef struct {
+    int n;
+    int nnz;
+    const int *rowptr;   /* n+1 */
+    const int *colind;   /* nnz, sorted within each row */
+    const void *vals;    /* nnz, dtype below */
+    int index_base;      /* 0 or 1 */
+    int dtype;           /* bpf_dtype; only BPF_F64 for the system matrix */
+} bpf_csr_desc;
+
+/* Keyword arguments of block_gmres (src/block_gmres.jl:142-145). */
+typedef struct {
+    int memory;              /* default 20 */
+    int restart;             /* bool */
+    int reorthogonalization; /* bool */
+    int ldiv;                /* bool: preconditioners applied with ldiv! (true) or mul! */
+    double atol;             /* default sqrt(eps) */
+    double rtol;             /* default sqrt(eps) */
+    int itmax;               /* 0 -> 2*div(n,p) */
+    double timemax;          /* seconds, <= 0 or inf -> no limit */
+    int verbose;             /* print every `verbose` iterations (host stdout) */
+    int history;             /* bool: record residual norms */
+} bpf_gmres_opts;
+
+/* Keyword arguments of block_bicgstab (src/block_bicgstab.jl:182-185). */
+typedef struct {
+    double atol;
+    double rtol;
+    int itmax;               /* 0 -> 2n */
+    double timemax;
+    int verbose;
+    int history;
+} bpf_bicgstab_opts;
+
+/* BlockGMRESStats / SimpleStats (src/block_utils.jl:62-68, src/block_bicgstab.jl:15-21). */
+typedef struct {
+    int niter;
+    int solved;              /* bool */
+    int status;              /* bpf_solve_status */
+    double timer;            /* seconds */
+    int n_residuals;         /* residual norms produced (may exceed the capacity) */
+    int residuals_capacity;  /* capacity of `residuals` */
+    double *residuals;       /* caller-owned HOST buffer or NULL */
+    int npass;               /* restart passes (GMRES) */
+} bpf_stats;
+
+/* ---- context ------------------------------------------------------------------------- */
+/* stream: a cudaStream_t (NULL = legacy default stream).  Replaces the implicit CUDA.jl
+ * task-local stream / library handles of src/BlockPowerFlow.jl:1-31. */
+BPF_API bpf_status bpf_ctx_create(bpf_ctx **ctx, void *stream);
+BPF_API bpf_status bpf_ctx_set_stream(bpf_ctx *ctx, void *stream);
+BPF_API bpf_status bpf_ctx_destroy(bpf_ctx *ctx);
+BPF_API const char *bpf_last_error(const bpf_ctx *ctx);
+BPF_API const char *bpf_solve_status_string(int status);
+/* Number of kernels this library launched on the context (a running counter). */
+BPF_API long long bpf_ctx_kernel_launches(const bpf_ctx *ctx);
+
+/* ---- sparse x dense block -------------------------------------------------------------- */
+/* Y = alpha*A*X + beta*Y: mul!(W, A, P) of src/block_gmres.jl:299 (CSR SpMM). */
+BPF_API bpf_status bpf_spmm(bpf_ctx *ctx, const bpf_csr_desc *A, int p, double alpha,
+                            const double *X, int ldx, double beta, double *Y, int ldy);
+
+/* Reduced QR of an n x p block, Q overwritten by the orthonormal factor and R (p x p, upper,
+ * ldr) written: householder!(Q, R, tau) of src/block_utils.jl:46-53.  Computed as shifted /
+ * plain Cholesky-QR2, so R's diagonal is positive (LAPACK's may be negative; Q and R differ from
+ * LAPACK's by the same diagonal +-1 scaling). */
+BPF_API bpf_status bpf_householder(bpf_ctx *ctx, int n, int p, double *Q, int ldq, double *R,
+                                   int ldr);
+
+/* ---- preconditioners ------------------------------------------------------------------- */
+/* ilu0(A, nrhs) -- src/preconditioners_nvidia.jl:42-47 (csrilu02 on A's pattern). */
+BPF_API bpf_status bpf_ilu0_create(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs,
+                                   int factor_dtype, bpf_prec **prec);
+/* ic0(A, nrhs) -- src/preconditioners_nvidia.jl:6-11 (csric02 on A's lower triangle). */
+BPF_API bpf_status bpf_ic0_create(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs,
+                                  int factor_dtype, bpf_prec **prec);
+/* New values on the same pattern (device pointer, nnz doubles), then refactor.  The
+ * reference rebuilds the preconditioner with ilu0(A) after each Jacobian update
+ * (benchmarks/benchmarks_nvidia.jl:44). */
+BPF_API bpf_status bpf_prec_refactor(bpf_prec *prec, const double *vals);
+/* ldiv!(Y, P, X): Y = U \ (L \ X) (ILU0) or Y = L' \ (L \ X) (IC0);
+ * src/preconditioners_nvidia.jl:13-35,49-71.  Y may equal X. */
+BPF_API bpf_status bpf_prec_apply(bpf_prec *prec, int p, const double *X, int ldx, double *Y,
+                                  int ldy);
+/* Copy the factor values (A's pattern, nnz doubles, device pointer) out: the P field of
+ * NVIDIA_ILU0 / NVIDIA_IC0 (src/preconditioners_nvidia.jl:1-4,37-40). */
+BPF_API bpf_status bpf_prec_factor_values(const bpf_prec *prec, double *vals);
+/* Number of dependency levels of the forward (L) and backward (U or L') solves. */
+BPF_API bpf_status bpf_prec_levels(const bpf_prec *prec, int *levels_lower, int *levels_upper);
+BPF_API bpf_status bpf_prec_destroy(bpf_prec *prec);
+
+/* ---- block Krylov solvers -------------------------------------------------------------- */
+/* block_gmres(A, B[, X0]; kwargs...) -> (X, stats): src/block_gmres.jl:127-154,170-411.
+ * X0 nullable (warm start).  M: left, N: right preconditioner, either nullable (= I). */
+BPF_API bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p,
+                                   const double *B, int ldb, double *X, int ldx,
+                                   const double *X0, int ldx0, const bpf_prec *M,
+                                   const bpf_prec *N, const bpf_gmres_opts *opts,
+                                   bpf_stats *stats);
+
+/* block_bicgstab(A, B; C=B, N, kwargs...) -> (X, stats): src/block_bicgstab.jl:182-299.
+ * C (shadow block) nullable -> B.  N: right preconditioner (nullable = I), applied as
+ * Y = N^{-1} P exactly as the reference's comment at :247 states. */
+BPF_API bpf_status bpf_block_bicgstab(bpf_ctx *ctx, const bpf_csr_desc *A, int p,
+                                      const double *B, int ldb, double *X, int ldx,
+                                      const double *C, int ldc, const bpf_prec *N,
+                                      const bpf_bicgstab_opts *opts, bpf_stats *stats);
+
+/* ---- refactorization (cusolverRF replacement) ------------------------------------------ */
+/* CusolverRfLU(A; ordering, tol, fast_mode) / CusolverRfLUBatch(A, batch; ...):
+ * src/cusolverRF.jl:222-301,336-419.  Host analysis (ordering + threshold-pivoted LU), then
+ * the device refactor.  batch >= 1 (1 = CusolverRfLU).  A zero pivot (|pivot| <= tol *
+ * max|A|) returns BPF_ERR_SINGULAR; the reference constructs a SingularException there but
+ * never throws it (:164-166). */
+BPF_API bpf_status bpf_rf_analyze(bpf_ctx *ctx, const bpf_csr_desc *A, int ordering,
+                                  double tol, int fast_mode, int batch, bpf_rf **rf);
+/* update!(rflu, A) / lu!(rflu, A): new values on A's pattern (device, nnz doubles), then the
+ * device refactor (src/cusolverRF.jl:304-314,334,422-434). */
+BPF_API bpf_status bpf_rf_refactor(bpf_rf *rf, const double *vals);
+/* rf_batch_refactor!(rflu, Anzval): replica r takes column r of the nnz x batch matrix
+ * `vals` (leading dimension ld) (src/cusolverRF.jl:472-481). */
+BPF_API bpf_status bpf_rf_refactor_batch(bpf_rf *rf, const double *vals, int ld);
+/* ldiv!(x, rflu, b) / ldiv!(rflu, x) / solve! (src/cusolverRF.jl:317-331,439-470): in place,
+ * X is n x nrhs (ldx).  Single mode solves every column with the one factorization
+ * (multi-RHS; the reference allows only nrhs = 1, :228-230).  Batch mode requires
+ * nrhs == batch and solves column r with replica r. */
+BPF_API bpf_status bpf_rf_solve(bpf_rf *rf, int nrhs, double *X, int ldx);
+/* nnz of L (strict lower) and U (incl. diagonal), and the host-side P/Q permutations
+ * (0-based, n ints each; nullable). */
+BPF_API bpf_status bpf_rf_info(const bpf_rf *rf, int *nnzL, int *nnzU, int *P, int *Q);
+/* cudestroy!(rflu) (src/cusolverRF.jl:17-22,54). */
+BPF_API bpf_status bpf_rf_destroy(bpf_rf *rf);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BPF_H_ */
