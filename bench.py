@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""RHS solves/s at a 1e-8 relative residual on one B200 (one JSON line on stdout).
+
+Workload (the 9,000-bus grid of the second benchmark configuration): a seeded synthetic
+Newton power-flow Jacobian with 9,000 buses (16,998 unknowns, ~121k nonzeros) and 64 Gaussian
+right-hand sides, solved by block-GMRES with a right ILU(0) preconditioner, no restart (as in
+benchmarks_nvidia.jl), atol 0, rtol 1e-8.  One step = ILU(0) numeric refactorization of the
+Jacobian's values + the block-GMRES solve; the sparsity analysis is done once at set-up, as a
+Newton loop would.  RHS solves/s = converged right-hand sides / time.
+
+  value : device-resident inputs, CUDA-event time of K steps (max over ranks), L2 flushed
+          between steps (256 MB write).
+  e2e   : the same step through the public Python API with pinned host buffers: Jacobian
+          values and B copied host->device and X device->host inside the timed region.
+  roofline : the kernel class with the largest share of device time, measured live with
+          CUDA events around each of its launches inside the timed region.
+  cpu_baseline : the C restatement of the reference's block-GMRES (oracle/) on the host's
+          cores, first iterations of the same solve, scaled to the whole solve by operation
+          count.
+
+`--impl reference` times that CPU restatement alone (the reference is Julia and cannot run
+here) on the same workload and prints the same metric with "impl":"reference".
+Multi-GPU (torchrun): every rank solves its own grid (seed offset by rank), no collective on
+the data path; value = all ranks' converged RHS / max-over-ranks time ("scaling": "weak").
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "blockpowerflow.jl_b200"))
+
+METRIC = "RHS solves/s at 1e-8 residual: mixed+learned vs plain FP64 block-GMRES, 1 B200"
+UNIT = "RHS solves/s"
+N_BUS, N_PV, P_RHS = 9000, 1000, 64
+RTOL = 1e-8
+ITMAX = 300
+CPU_SAMPLE_ITERS = (4, 10)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+
+        def reader():
+            for line in self.proc.stdout:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    self.samples.append(parts)
+
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if s[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def make_workload(rank):
+    from blockpowerflow_b200 import grid as g
+
+    grid = g.make_grid(N_BUS, N_PV, seed=rank)
+    J = g.jacobian(grid)
+    B = g.gaussian_rhs(J.shape[0], P_RHS, seed=1000 + rank)
+    return J, B
+
+
+def cpu_baseline(J, B, gpu_iters, threads):
+    """Oracle block-GMRES (C, OpenMP) on the host: two short runs give the cost per iteration
+    (constant part + part growing with the basis), extrapolated to `gpu_iters` iterations."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+
+    O.set_threads(threads)
+    t0 = time.time()
+    F = O.ilu0(J)
+    t_factor = time.time() - t0
+    times = []
+    for it in CPU_SAMPLE_ITERS:
+        t0 = time.time()
+        O.block_gmres(J, B, N=(1, F), memory=it, restart=False, atol=0.0, rtol=RTOL, itmax=it)
+        times.append(time.time() - t0)
+    (k1, k2), (t1, t2) = CPU_SAMPLE_ITERS, times
+    # T(k) = a k + b k (k + 1) / 2  (SpMM / ILU0 / QR per iteration + Gram-Schmidt over k blocks)
+    A_ = np.array([[k1, k1 * (k1 + 1) / 2], [k2, k2 * (k2 + 1) / 2]])
+    a, b = np.linalg.solve(A_, np.array([t1, t2]))
+    a, b = max(a, 0.0), max(b, 0.0)
+    K = gpu_iters
+    t_full = t_factor + a * K + b * K * (K + 1) / 2
+    return {"value": B.shape[1] / t_full, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"oracle block-GMRES + ILU0 on the same {J.shape[0]}-unknown system, "
+                       f"{B.shape[1]} RHS: runs of {k1} and {k2} iterations "
+                       f"({t1:.2f} s, {t2:.2f} s) fit T(k)=a k + b k(k+1)/2, extrapolated to the "
+                       f"{K} iterations the solve needs, plus the ILU0 factorization ({t_factor:.2f} s)"),
+            "seconds_per_solve": t_full}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    J, B = make_workload(0)
+    threads = os.cpu_count() or 1
+    vals = []
+    cb = None
+    iters = args.ref_iters
+    for s in range(args.warmup + args.steps):
+        cb = cpu_baseline(J, B, iters, threads)
+        if s >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.mean(vals)
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * P_RHS / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_config(world),
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(world):
+    return {"workload": "grid9k_p64_block_gmres_ilu0", "n_bus": N_BUS, "n_pv": N_PV,
+            "unknowns": 16998, "rhs": P_RHS, "solver": "block_gmres(restart=false, itmax=300)",
+            "preconditioner": "ILU0 (right, ldiv), FP64 factors", "rtol": RTOL,
+            "step": "ILU0 numeric refactor + block-GMRES solve", "l2": "flushed between steps",
+            "parallelism": f"replicas x{world} (independent grids)"}
+
+
+def kernel_only(name, reps):
+    """A few launches of one kernel on a case whose blocks exceed L2, for ncu captures:
+    70,000-bus grid (134,998 unknowns, ~980k nonzeros), 128 right-hand sides."""
+    import numpy as np
+    import torch
+
+    import blockpowerflow_b200 as bpf
+
+    J = bpf.grid.preset_jacobian("case70k", 0)
+    n = J.shape[0]
+    p = 128
+    A = bpf.CuSparseMatrixCSR.from_scipy(J)
+    X = bpf.colmajor(torch.randn(n, p, dtype=torch.float64, device="cuda"))
+    Y = bpf.empty_colmajor(n, p)
+    if name in ("trsv", "factor"):
+        P = bpf.ilu0(A, p)
+    for _ in range(reps):
+        if name == "trsv":
+            bpf.ldiv_(Y, P, X)
+        elif name == "spmm":
+            bpf.mul(A, X, Y=Y)
+        elif name == "factor":
+            P.refactor(A.nzVal)
+        elif name == "gram":
+            bpf.householder(X[:, :64])
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_only": name, "n": n, "p": p, "reps": reps}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--kernel-only", choices=["trsv", "spmm", "factor", "gram"], default=None,
+                    help="launch one kernel a few times on a 135k-unknown case (for ncu)")
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-iters", type=int, default=69,
+                    help="iterations the reference arm extrapolates to (the GPU solve's count)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.kernel_only:
+        kernel_only(args.kernel_only, args.reps)
+        return
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_
+
+        dist = dist_
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import numpy as np
+    import torch
+
+    import blockpowerflow_b200 as bpf
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    J, B = make_workload(rank)
+    n = J.shape[0]
+    A = bpf.CuSparseMatrixCSR.from_scipy(J, device=dev)
+    vals_dev = A.nzVal.clone()
+    Bd = bpf.colmajor(torch.as_tensor(B, device=dev))
+    N = bpf.ilu0(A, P_RHS)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    # pinned host buffers for the end-to-end measurement
+    vals_h = torch.as_tensor(J.data.astype(np.float64)).pin_memory()
+    B_h = torch.as_tensor(np.ascontiguousarray(B.T)).pin_memory()   # column-major n x p
+    X_h = torch.empty((P_RHS, n), dtype=torch.float64).pin_memory()
+
+    def solve():
+        N.refactor(A.nzVal)
+        return bpf.block_gmres(A, Bd, N=N, ldiv=True, restart=False, memory=ITMAX, atol=0.0,
+                               rtol=RTOL, itmax=ITMAX)
+
+    def step_e2e():
+        A.nzVal.copy_(vals_h, non_blocking=True)
+        Bh_dev = torch.empty((P_RHS, n), dtype=torch.float64, device=dev)
+        Bh_dev.copy_(B_h, non_blocking=True)  # row-major p x n == column-major n x p
+        N.refactor(A.nzVal)
+        X, st = bpf.block_gmres(A, Bh_dev.t(), N=N, ldiv=True, restart=False, memory=ITMAX,
+                                atol=0.0, rtol=RTOL, itmax=ITMAX)
+        X_h.copy_(X.t(), non_blocking=False)
+        return st
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    for _ in range(max(3, args.warmup)):
+        X, st = solve()
+        step_e2e()
+    torch.cuda.synchronize()
+    iters = st.niter
+
+    # ---- device-resident timed region --------------------------------------------------
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    l0 = bpf.kernel_launches()
+    bpf._lib.set_timing(True)
+    barrier()
+    if sampler:
+        sampler.start()
+    ev = []
+    solved_rhs = 0
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        X, st = solve()
+        e1.record()
+        ev.append((e0, e1))
+        solved_rhs += P_RHS if st.solved else 0
+    barrier()
+    clocks = sampler.stop() if sampler else None
+    launches = bpf.kernel_launches() - l0
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    kern = {}
+    for kc in ("spmm", "trsv", "factor", "gram", "tsmm", "small"):
+        ms, cnt, by, fl = bpf._lib.kernel_time(kc)
+        kern[kc] = {"ms": ms, "launches": cnt, "bytes": by, "flops": fl}
+    bpf._lib.set_timing(False)
+    t_max = max_over_ranks(t_ms)
+    total_rhs = sum_over_ranks(solved_rhs)
+    value = total_rhs / (t_max / 1e3)
+    # true residual of the last solve, every column
+    R = B - J @ X.cpu().numpy()
+    col_rel = np.linalg.norm(R, axis=0) / np.linalg.norm(B, axis=0)
+    rel = float(np.linalg.norm(R) / np.linalg.norm(B))
+
+    # ---- end-to-end timed region ---------------------------------------------------------
+    barrier()
+    e2e_t = 0.0
+    e2e_rhs = 0
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st2 = step_e2e()
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_t += e0.elapsed_time(e1)
+        e2e_rhs += P_RHS if st2.solved else 0
+    e2e_t = max_over_ranks(e2e_t)
+    e2e_val = sum_over_ranks(e2e_rhs) / (e2e_t / 1e3)
+
+    # ---- roofline of the dominant kernel class -------------------------------------------
+    hbm, hbm_src = peaks()
+    dom = max(kern, key=lambda k: kern[k]["ms"])
+    total_kernel_ms = sum(v["ms"] for v in kern.values())
+    breakdown = {}
+    for k, v in kern.items():
+        if v["launches"] == 0:
+            continue
+        s = v["ms"] / 1e3
+        breakdown[k] = {"share": v["ms"] / max(t_ms, 1e-9), "launches": v["launches"],
+                        "avg_us": 1e3 * v["ms"] / v["launches"],
+                        "GBps": v["bytes"] / s / 1e9 if v["bytes"] else None,
+                        "TFLOPs": v["flops"] / s / 1e12 if v["flops"] else None}
+    # HBM-bound classes are the sparse kernels; Gram / tsmm are FP64-FMA bound at p = 64.
+    hbm_classes = ("trsv", "spmm", "factor")
+    rk = dom if dom in hbm_classes else max(hbm_classes, key=lambda k: kern[k]["ms"])
+    v = kern[rk]
+    ach = v["bytes"] / (v["ms"] / 1e3) / 1e9 if v["ms"] > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": rk, "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "peak_source": hbm_src,
+                "bytes_per_launch": v["bytes"] / max(v["launches"], 1),
+                "avg_launch_us": 1e3 * v["ms"] / max(v["launches"], 1),
+                "traffic": None, "dominant_class": dom,
+                "dominant_share_of_device_time": kern[dom]["ms"] / max(t_ms, 1e-9)}
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(J, B, iters, os.cpu_count() or 1)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": t_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(world),
+        "iterations": iters, "relres": rel, "max_column_relres": float(col_rel.max()),
+        "solved_fraction": solved_rhs / (P_RHS * args.steps),
+        "e2e": {"value": e2e_val, "unit": UNIT,
+                "h2d_bytes_per_step": int(8 * (J.nnz + n * P_RHS)),
+                "d2h_bytes_per_step": int(8 * n * P_RHS)},
+        "gpu_launches": int(launches), "roofline": roofline, "kernels": breakdown,
+        "cpu_baseline": cb, "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

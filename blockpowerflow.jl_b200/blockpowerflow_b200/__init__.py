@@ -4,6 +4,7 @@ Python mirror of the reference's Julia API (module BlockPowerFlow, src/BlockPowe
 block_gmres, block_bicgstab, ilu0, ic0, ldiv!, CUSOLVERRF.  Every call runs in libbpf.so
 (hand-written sm_100a kernels); there is no CPU fallback.
 """
+from . import cusolverrf as CUSOLVERRF
 from . import grid
 from ._lib import (BPFError, DimensionMismatch, SingularException, exported_symbols,
                    kernel_launches)
@@ -17,5 +18,5 @@ __all__ = [
     "block_gmres", "block_bicgstab", "BlockGMRESStats", "SimpleStats", "ilu0", "ic0", "ldiv_",
     "ldiv", "NVIDIA_ILU0", "NVIDIA_IC0", "CuSparseMatrixCSR", "mul", "householder", "colmajor",
     "empty_colmajor", "BPFError", "DimensionMismatch", "SingularException", "grid",
-    "exported_symbols", "kernel_launches",
+    "exported_symbols", "kernel_launches", "CUSOLVERRF",
 ]

@@ -77,6 +77,9 @@ SIGNATURES = {
     "bpf_last_error": (C.c_char_p, [_P]),
     "bpf_solve_status_string": (C.c_char_p, [_I]),
     "bpf_ctx_kernel_launches": (C.c_longlong, [_P]),
+    "bpf_ctx_set_timing": (_I, [_P, _I]),
+    "bpf_ctx_kernel_time": (_I, [_P, _I, C.POINTER(_D), C.POINTER(C.c_longlong),
+                                 C.POINTER(_D), C.POINTER(_D)]),
     "bpf_spmm": (_I, [_P, C.POINTER(CsrDesc), _I, _D, _P, _I, _D, _P, _I]),
     "bpf_householder": (_I, [_P, _I, _I, _P, _I, _P, _I]),
     "bpf_ilu0_create": (_I, [_P, C.POINTER(CsrDesc), _I, _I, C.POINTER(_P)]),
@@ -170,3 +173,20 @@ def check(status: int, ctx) -> None:
 
 def kernel_launches(device=None) -> int:
     return int(load().bpf_ctx_kernel_launches(context(device)))
+
+
+KERNEL_CLASSES = {"spmm": 0, "trsv": 1, "factor": 2, "gram": 3, "tsmm": 4, "small": 5}
+
+
+def set_timing(on: bool, device=None) -> None:
+    ctx = context(device)
+    check(load().bpf_ctx_set_timing(ctx, int(bool(on))), ctx)
+
+
+def kernel_time(kernel_class: str, device=None):
+    """(total ms, launches, algorithmic bytes, flops) of a kernel class since set_timing(True)."""
+    ctx = context(device)
+    t, c, b, f = C.c_double(), C.c_longlong(), C.c_double(), C.c_double()
+    check(load().bpf_ctx_kernel_time(ctx, KERNEL_CLASSES[kernel_class], C.byref(t), C.byref(c),
+                                     C.byref(b), C.byref(f)), ctx)
+    return t.value, c.value, b.value, f.value

@@ -50,6 +50,18 @@ void *ws_get(bpf_ctx *ctx, int slot, size_t bytes, bpf_status *st) {
     return p;
 }
 
+cudaEvent_t timing_event(bpf_ctx *ctx) {
+    if (ctx->event_next >= ctx->event_pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        ctx->event_pool.push_back(e);
+    }
+    return ctx->event_pool[ctx->event_next++];
+}
+
 bpf_status reset_dev_status(bpf_ctx *ctx) {
     BPF_CUDA(ctx, cudaMemsetAsync(ctx->dstat, 0, sizeof(DevStatus), ctx->stream));
     return BPF_SUCCESS;
@@ -209,6 +221,7 @@ bpf_status bpf_ctx_set_stream(bpf_ctx *ctx, void *stream) {
 bpf_status bpf_ctx_destroy(bpf_ctx *ctx) {
     if (!ctx) return BPF_SUCCESS;
     cudaStreamSynchronize(ctx->stream);
+    for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     for (int s = 0; s < WS_COUNT; s++)
         if (ctx->ws[s]) cudaFree(ctx->ws[s]);
     cudaFree(ctx->dstat);
@@ -223,6 +236,37 @@ const char *bpf_last_error(const bpf_ctx *ctx) {
 }
 
 long long bpf_ctx_kernel_launches(const bpf_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+bpf_status bpf_ctx_set_timing(bpf_ctx *ctx, int on) {
+    if (!ctx) return BPF_ERR_INVALID_VALUE;
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->timed.clear();
+    ctx->event_next = 0;
+    ctx->timing = on != 0;
+    return BPF_SUCCESS;
+}
+
+bpf_status bpf_ctx_kernel_time(bpf_ctx *ctx, int kc, double *total_ms, long long *launches,
+                               double *bytes, double *flops) {
+    if (!ctx || kc < 0 || kc >= BPF_KC_COUNT) return BPF_ERR_INVALID_VALUE;
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    double t = 0.0, by = 0.0, fl = 0.0;
+    long long c = 0;
+    for (const auto &r : ctx->timed) {
+        if (r.kc != kc) continue;
+        float ms = 0.f;
+        BPF_CUDA(ctx, cudaEventElapsedTime(&ms, r.a, r.b));
+        t += ms;
+        by += r.bytes;
+        fl += r.flops;
+        c++;
+    }
+    if (total_ms) *total_ms = t;
+    if (launches) *launches = c;
+    if (bytes) *bytes = by;
+    if (flops) *flops = fl;
+    return BPF_SUCCESS;
+}
 
 const char *bpf_solve_status_string(int status) {
     switch (status) {
@@ -254,7 +298,7 @@ bpf_status bpf_spmm(bpf_ctx *ctx, const bpf_csr_desc *A, int p, double alpha, co
         int pc = std::min(chunk, p - c0);
         BPF_TRY(colmajor_to_rowmajor(ctx, n, pc, X + (size_t)c0 * ldx, ldx, xr));
         if (beta != 0.0) BPF_TRY(colmajor_to_rowmajor(ctx, n, pc, Y + (size_t)c0 * ldy, ldy, yr));
-        BPF_TRY(spmm_rowmajor(ctx, n, A->rowptr, A->colind, (const double *)A->vals, A->index_base,
+        BPF_TRY(spmm_rowmajor(ctx, n, A->nnz, A->rowptr, A->colind, (const double *)A->vals, A->index_base,
                               pc, alpha, xr, beta, yr, nullptr));
         BPF_TRY(rowmajor_to_colmajor(ctx, n, pc, yr, Y + (size_t)c0 * ldy, ldy));
     }

@@ -305,10 +305,13 @@ extern "C" bpf_status bpf_block_bicgstab(bpf_ctx *ctx, const bpf_csr_desc *A, in
                 BPF_TRY(prec_apply_rowmajor(ctx, N, p, P, Yb, act));
                 Yp = Yb;
             }
-            BPF_TRY(spmm_rowmajor(ctx, n, rp, ci, av, base, p, 1.0, Yp, 0.0, V, nullptr, act));  // :365
+            BPF_TRY(spmm_rowmajor(ctx, n, A->nnz, rp, ci, av, base, p, 1.0, Yp, 0.0, V, nullptr, act));  // :365
             BPF_TRY(gram(ctx, n, p, 1, Cm, 0, V, K, 1.0, false, st));      // :366
             BPF_TRY(gram(ctx, n, p, 1, Cm, 0, R, D, 1.0, false, st));      // :367
-            small_qr_solve_kernel<<<1, 1024, 0, ctx->stream>>>(p, K, Kf, tau, D, alpha, 0, st);  // :368-371
+            {
+                KScope ks(ctx, BPF_KC_SMALL);
+                small_qr_solve_kernel<<<1, 1024, 0, ctx->stream>>>(p, K, Kf, tau, D, alpha, 0, st);  // :368-371
+            }
             BPF_LAUNCHED(ctx);
             BPF_TRY(tsmm(ctx, n, p, 1, V, 0, alpha, 0, -1.0, R, 1.0, U, st));   // :372-373
             BPF_TRY(tsmm(ctx, n, p, 1, Yp, 0, alpha, 0, 1.0, nullptr, 0.0, R, st));  // :374
@@ -318,7 +321,7 @@ extern "C" bpf_status bpf_block_bicgstab(bpf_ctx *ctx, const bpf_csr_desc *A, in
                 BPF_TRY(prec_apply_rowmajor(ctx, N, p, U, Yb, act));
                 Yu = Yb;
             }
-            BPF_TRY(spmm_rowmajor(ctx, n, rp, ci, av, base, p, 1.0, Yu, 0.0, Q, nullptr, act));  // :377
+            BPF_TRY(spmm_rowmajor(ctx, n, A->nnz, rp, ci, av, base, p, 1.0, Yu, 0.0, Q, nullptr, act));  // :377
             dot2_partial_kernel<<<nparts, 256, 0, ctx->stream>>>(np, Q, U, part, st);        // :378
             BPF_LAUNCHED(ctx);
             omega_kernel<<<1, 256, 0, ctx->stream>>>(nparts, part, st);

@@ -66,6 +66,12 @@ struct bpf_ctx {
     int max_smem_optin = 0;
     std::string last_error;
     long long launches = 0;
+    // per-kernel-class event timing (bpf_ctx_set_timing)
+    bool timing = false;
+    std::vector<cudaEvent_t> event_pool;
+    size_t event_next = 0;
+    struct TimedLaunch { int kc; cudaEvent_t a, b; double bytes, flops; };
+    std::vector<TimedLaunch> timed;
     bpf::DevStatus *dstat = nullptr;   // device
     bpf::DevStatus *hstat = nullptr;   // pinned host mirror
     void *ws[bpf::WS_COUNT] = {};
@@ -103,6 +109,31 @@ bpf_status reset_dev_status(bpf_ctx *ctx);
     } while (0)
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Records a CUDA event pair around one launch when the context's timing is on.
+cudaEvent_t timing_event(bpf_ctx *ctx);
+struct KScope {
+    bpf_ctx *ctx;
+    int kc;
+    double bytes, flops;
+    cudaEvent_t a = nullptr;
+    KScope(bpf_ctx *c, int k, double algo_bytes = 0.0, double algo_flops = 0.0)
+        : ctx(c), kc(k), bytes(algo_bytes), flops(algo_flops) {
+        if (ctx->timing) {
+            a = timing_event(ctx);
+            if (a) cudaEventRecord(a, ctx->stream);
+        }
+    }
+    ~KScope() {
+        if (a) {
+            cudaEvent_t b = timing_event(ctx);
+            if (b) {
+                cudaEventRecord(b, ctx->stream);
+                ctx->timed.push_back({kc, a, b, bytes, flops});
+            }
+        }
+    }
+};
 
 // ------------------------------------------------------------------------------------
 // device helpers
@@ -191,11 +222,11 @@ bpf_status rowmajor_to_colmajor(bpf_ctx *ctx, int n, int p, const double *src, d
 
 // CSR SpMM on row-major blocks: Y = alpha*A*X + beta*Y, or (residual) Y = B - A*X when
 // B != nullptr.  base = index base of the CSR arrays.
-bpf_status spmm_rowmajor(bpf_ctx *ctx, int n, const int *rp, const int *ci, const double *av,
-                         int base, int p, double alpha, const double *X, double beta,
-                         double *Y, const double *B, const int *gate = nullptr);
+bpf_status spmm_rowmajor(bpf_ctx *ctx, int n, long long nnz, const int *rp, const int *ci,
+                         const double *av, int base, int p, double alpha, const double *X,
+                         double beta, double *Y, const double *B, const int *gate = nullptr);
 // Same with an FP32 input block (mixed-precision path): Y = A*X.
-bpf_status spmm_rowmajor_f32x(bpf_ctx *ctx, int n, const int *rp, const int *ci,
+bpf_status spmm_rowmajor_f32x(bpf_ctx *ctx, int n, long long nnz, const int *rp, const int *ci,
                               const double *av, int base, int p, const float *X, double *Y,
                               const int *gate = nullptr);
 

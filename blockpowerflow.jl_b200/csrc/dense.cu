@@ -122,6 +122,7 @@ bpf_status gram(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
     double *partial = (double *)ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)nchunks * nb * p * p, &s);
     if (!partial) return s;
     dim3 grid(nchunks, nb, tiles);
+    KScope ks(ctx, BPF_KC_GRAM, 8.0 * n * p * (nb + (A == B ? 0 : 1)), 2.0 * n * p * (double)p * nb);
     if (GT == 16)
         gram_partial_kernel<16><<<grid, 256, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
                                                                 rows_per_chunk, st, qr_gate, gate2);
@@ -216,6 +217,8 @@ bpf_status tsmm(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
     if (n <= 0 || p <= 0) return BPF_SUCCESS;
     const int GT = p <= 16 ? 16 : (p <= 32 ? 32 : 64);
     dim3 grid(ceil_div(n, kTsmmRows), ceil_div(p, GT));
+    KScope ks(ctx, BPF_KC_TSMM, 8.0 * n * p * (nb + 1 + ((Cin && beta != 0.0) ? 1 : 0)),
+              2.0 * n * p * (double)p * nb);
     if (GT == 16)
         tsmm_kernel<16><<<grid, 256, 0, ctx->stream>>>(n, p, nb, A, strideA, S, strideS, alpha, Cin,
                                                         beta, Out, st, nb_dev, qr_gate, gate2);
@@ -366,6 +369,7 @@ static bpf_status launch_chol(bpf_ctx *ctx, int n, int p, const double *G, doubl
         BPF_CUDA(ctx, cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem));
     }
+    KScope ks(ctx, BPF_KC_SMALL);
     chol_kernel<<<1, 1024, smem, ctx->stream>>>(n, p, G, Rinv, Racc, Rtmp, pass, st, gate, gate2,
                                                 shift_flag, reorth_flag, ctx->dstat);
     BPF_LAUNCHED(ctx);

@@ -449,7 +449,7 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
     const bool warm = X0 != nullptr;
     if (warm) {
         BPF_TRY(colmajor_to_rowmajor(ctx, n, p, X0, ldx0, dX));
-        BPF_TRY(spmm_rowmajor(ctx, n, rp, ci, av, base, p, 1.0, dX, 0.0, W, Bi));
+        BPF_TRY(spmm_rowmajor(ctx, n, A->nnz, rp, ci, av, base, p, 1.0, dX, 0.0, W, Bi));
         if (restart) BPF_CUDA(ctx, cudaMemcpyAsync(Xi, dX, sizeof(double) * np, cudaMemcpyDeviceToDevice, ctx->stream));
     } else {
         BPF_CUDA(ctx, cudaMemcpyAsync(W, Bi, sizeof(double) * np, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -478,7 +478,7 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
         if (restart) {
             BPF_CUDA(ctx, cudaMemsetAsync(dX, 0, sizeof(double) * np, ctx->stream));
             if (npass >= 1) {                                               // :267-271
-                BPF_TRY(spmm_rowmajor(ctx, n, rp, ci, av, base, p, 1.0, Xi, 0.0, W, Bi));
+                BPF_TRY(spmm_rowmajor(ctx, n, A->nnz, rp, ci, av, base, p, 1.0, Xi, 0.0, W, Bi));
                 if (M) BPF_TRY(prec_apply_rowmajor(ctx, M, p, W, Qm));
             }
         }
@@ -508,7 +508,7 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
                     BPF_TRY(prec_apply_rowmajor(ctx, N, p, Vk, Pm, &st->active));
                     Pk = Pm;
                 }
-                BPF_TRY(spmm_rowmajor(ctx, n, rp, ci, av, base, p, 1.0, Pk, 0.0, W, nullptr, &st->active));
+                BPF_TRY(spmm_rowmajor(ctx, n, A->nnz, rp, ci, av, base, p, 1.0, Pk, 0.0, W, nullptr, &st->active));
                 double *Qk = W;
                 if (M) {                                                     // :300
                     BPF_TRY(prec_apply_rowmajor(ctx, M, p, W, Qm, &st->active));
@@ -532,6 +532,7 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
                     BPF_TRY(cholqr(ctx, n, p, Qk, Vn, C2, Tq, st, rg, &st->qr_shift2, nullptr));
                     BPF_TRY(reorth_fold(ctx, p, kk, Psi, Psi2buf, Cm, C2, Cm, fold_scr, st, rg));
                 }
+                KScope ks(ctx, BPF_KC_SMALL);
                 hess_apply_kernel<<<p, 256, sizeof(double) * 4 * p, ctx->stream>>>(p, kk, g.Rblk, g.HY, st);
                 BPF_LAUNCHED(ctx);
                 hess_factor_kernel<<<1, 1024, 0, ctx->stream>>>(p, kk, g.Rblk, g.HY, tau_cur, g.Z, Cm, st,

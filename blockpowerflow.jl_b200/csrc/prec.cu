@@ -361,6 +361,10 @@ bpf_status factor_numeric(bpf_ctx *ctx, bpf_prec *P) {
     int grid = 1;
     BPF_TRY(coop_grid(ctx, factor_coop_kernel, 256, 0, want, &grid));
     void *args[] = {&a};
+    // Algorithmic bytes: factor values read and written once, the pattern, and the update
+    // pairs' two indices; flops: two per update pair.
+    KScope ks(ctx, BPF_KC_FACTOR, 16.0 * P->nnz + 4.0 * P->nnz + 8.0 * (P->n + 1) + 8.0 * P->npairs,
+              2.0 * P->npairs);
     BPF_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)factor_coop_kernel, dim3(grid),
                                               dim3(256), args, 0, ctx->stream));
     BPF_LAUNCHED(ctx);
@@ -464,6 +468,14 @@ static bpf_status launch_trsv2(bpf_ctx *ctx, const TriDev &t0, const TriDev &t1,
     TriKernelArgs a0 = t0.args(), a1 = t1.args();
     DevStatus *ds = ctx->dstat;
     void *args[] = {&a0, &a1, &p, (void *)&X, &Y, &ds, (void *)&gate};
+    // Algorithmic bytes: (4 + sizeof(TF)) per off-diagonal entry of both factors, the
+    // diagonal inverses, row pointers and row ids, and 4 n p vector values (read X, write Y,
+    // read and write Y in the backward sweep).
+    const double fb = (4.0 + sizeof(TF)) * ((double)t0.nnz + t1.nnz) + sizeof(TF) * (double)t0.n +
+                      16.0 * (t0.n + 1) + 8.0 * t0.n;
+    const double vb = (double)t0.n * p * ((IN_F32 ? 4.0 : 8.0) + 2.0 * (OUT_F32 ? 4.0 : 8.0) +
+                                          (OUT_F32 ? 4.0 : 8.0));
+    KScope ks(ctx, BPF_KC_TRSV, fb + vb, 2.0 * ((double)t0.nnz + t1.nnz + t0.n) * p);
     BPF_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)kern, dim3(grid), dim3(threads), args, 0,
                                               ctx->stream));
     BPF_LAUNCHED(ctx);

@@ -69,7 +69,7 @@ spmm_rm_kernel(int n, const int *__restrict__ rp, const int *__restrict__ ci,
 }
 
 template <int G, int CPL, typename TX>
-static bpf_status launch_spmm(bpf_ctx *ctx, int n, const int *rp, const int *ci,
+static bpf_status launch_spmm(bpf_ctx *ctx, int n, long long nnz, const int *rp, const int *ci,
                               const double *av, int base, int p, double alpha, const TX *X,
                               double beta, double *Y, const double *B, const int *gate) {
     const int threads = 256;
@@ -77,6 +77,10 @@ static bpf_status launch_spmm(bpf_ctx *ctx, int n, const int *rp, const int *ci,
     long long blocks_needed = ceil_div(n, groups);
     int blocks = (int)std::min<long long>(blocks_needed, (long long)ctx->num_sms * 16);
     if (blocks < 1) blocks = 1;
+    const double np = (double)n * p;
+    const double bytes = 12.0 * nnz + 4.0 * (n + 1) + sizeof(TX) * np + 8.0 * np +
+                         ((B || beta != 0.0) ? 8.0 * np : 0.0);
+    KScope ks(ctx, BPF_KC_SPMM, bytes, 2.0 * nnz * p);
     spmm_rm_kernel<G, CPL, TX><<<blocks, threads, 0, ctx->stream>>>(n, rp, ci, av, base, p, alpha,
                                                                     X, beta, Y, B, gate);
     BPF_LAUNCHED(ctx);
@@ -84,36 +88,36 @@ static bpf_status launch_spmm(bpf_ctx *ctx, int n, const int *rp, const int *ci,
 }
 
 template <typename TX>
-static bpf_status spmm_dispatch(bpf_ctx *ctx, int n, const int *rp, const int *ci,
+static bpf_status spmm_dispatch(bpf_ctx *ctx, int n, long long nnz, const int *rp, const int *ci,
                                 const double *av, int base, int p, double alpha, const TX *X,
                                 double beta, double *Y, const double *B, const int *gate) {
     if (n == 0 || p == 0) return BPF_SUCCESS;
-    if (p <= 4) return launch_spmm<4, 1>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
-    if (p <= 8) return launch_spmm<8, 1>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
-    if (p <= 16) return launch_spmm<16, 1>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
-    if (p <= 32) return launch_spmm<32, 1>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
-    if (p <= 64) return launch_spmm<32, 2>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
-    if (p <= 128) return launch_spmm<32, 4>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
-    if (p <= 256) return launch_spmm<32, 8>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
-    return launch_spmm<32, 16>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    if (p <= 4) return launch_spmm<4, 1>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    if (p <= 8) return launch_spmm<8, 1>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    if (p <= 16) return launch_spmm<16, 1>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    if (p <= 32) return launch_spmm<32, 1>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    if (p <= 64) return launch_spmm<32, 2>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    if (p <= 128) return launch_spmm<32, 4>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    if (p <= 256) return launch_spmm<32, 8>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    return launch_spmm<32, 16>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
 }
 
-bpf_status spmm_rowmajor(bpf_ctx *ctx, int n, const int *rp, const int *ci, const double *av,
-                         int base, int p, double alpha, const double *X, double beta,
-                         double *Y, const double *B, const int *gate) {
+bpf_status spmm_rowmajor(bpf_ctx *ctx, int n, long long nnz, const int *rp, const int *ci,
+                         const double *av, int base, int p, double alpha, const double *X,
+                         double beta, double *Y, const double *B, const int *gate) {
     if (p > 512) {
         return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "spmm: p=%d > 512 right-hand sides", p);
     }
-    return spmm_dispatch<double>(ctx, n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    return spmm_dispatch<double>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
 }
 
-bpf_status spmm_rowmajor_f32x(bpf_ctx *ctx, int n, const int *rp, const int *ci,
+bpf_status spmm_rowmajor_f32x(bpf_ctx *ctx, int n, long long nnz, const int *rp, const int *ci,
                               const double *av, int base, int p, const float *X, double *Y,
                               const int *gate) {
     if (p > 512) {
         return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "spmm: p=%d > 512 right-hand sides", p);
     }
-    return spmm_dispatch<float>(ctx, n, rp, ci, av, base, p, 1.0, X, 0.0, Y, nullptr, gate);
+    return spmm_dispatch<float>(ctx, n, nnz, rp, ci, av, base, p, 1.0, X, 0.0, Y, nullptr, gate);
 }
 
 // ------------------------------------------------------------------------------------

@@ -1,0 +1,273 @@
+# Julia host binding of libbpf.so: the reference's API (module BlockPowerFlow) on top of the
+# C ABI in include/bpf.h.  Same function names, keyword arguments, defaults, stats types and
+# error behaviour as src/block_gmres.jl, src/block_bicgstab.jl, src/preconditioners_nvidia.jl
+# and src/cusolverRF.jl; the arithmetic runs in the library's sm_100a kernels.
+#
+# Device pointers come from CUDA.jl arrays; the library works on the CUDA.jl task stream.
+# CuSparseMatrixCSR{Float64,Cint} is passed as it is (1-based, index_base = 1).
+module BlockPowerFlowB200
+
+using LinearAlgebra
+using CUDA
+using CUDA.CUSPARSE
+
+import LinearAlgebra: ldiv!
+
+export block_gmres, block_bicgstab, ilu0, ic0, CUSOLVERRF
+
+const libbpf = joinpath(@__DIR__, "..", "lib", "libbpf.so")
+
+struct CsrDesc
+    n::Cint
+    nnz::Cint
+    rowptr::CuPtr{Cint}
+    colind::CuPtr{Cint}
+    vals::CuPtr{Cdouble}
+    index_base::Cint
+    dtype::Cint
+end
+
+struct GmresOpts
+    memory::Cint
+    restart::Cint
+    reorthogonalization::Cint
+    ldiv::Cint
+    atol::Cdouble
+    rtol::Cdouble
+    itmax::Cint
+    timemax::Cdouble
+    verbose::Cint
+    history::Cint
+end
+
+struct BicgstabOpts
+    atol::Cdouble
+    rtol::Cdouble
+    itmax::Cint
+    timemax::Cdouble
+    verbose::Cint
+    history::Cint
+end
+
+mutable struct CStats
+    niter::Cint
+    solved::Cint
+    status::Cint
+    timer::Cdouble
+    n_residuals::Cint
+    residuals_capacity::Cint
+    residuals::Ptr{Cdouble}
+    npass::Cint
+end
+
+# BlockGMRESStats (src/block_utils.jl:62-68) and SimpleStats (src/block_bicgstab.jl:15-21)
+mutable struct BlockGMRESStats{T}
+    niter::Int
+    solved::Bool
+    residuals::Vector{T}
+    timer::Float64
+    status::String
+end
+mutable struct SimpleStats{T}
+    niter::Int
+    solved::Bool
+    residuals::Vector{T}
+    timer::Float64
+    status::String
+end
+
+const _ctx = Ref{Ptr{Cvoid}}(C_NULL)
+function ctx()
+    if _ctx[] == C_NULL
+        r = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:bpf_ctx_create, libbpf), Cint, (Ref{Ptr{Cvoid}}, Ptr{Cvoid}), r,
+                    CUDA.stream().handle))
+        _ctx[] = r[]
+    end
+    ccall((:bpf_ctx_set_stream, libbpf), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), _ctx[], CUDA.stream().handle)
+    return _ctx[]
+end
+
+function check(st::Cint)
+    st == 0 && return nothing
+    msg = _ctx[] == C_NULL ? "libbpf status $st" :
+          unsafe_string(ccall((:bpf_last_error, libbpf), Cstring, (Ptr{Cvoid},), _ctx[]))
+    st == 2 && throw(DimensionMismatch(msg))
+    st == 5 && throw(SingularException(0))
+    error(msg)
+end
+
+desc(A::CuSparseMatrixCSR{Float64,Cint}) =
+    CsrDesc(size(A, 1), nnz(A), pointer(A.rowPtr), pointer(A.colVal), pointer(A.nzVal), 1, 0)
+
+status_string(code) = unsafe_string(ccall((:bpf_solve_status_string, libbpf), Cstring, (Cint,), code))
+
+# ---- preconditioners (src/preconditioners_nvidia.jl) -----------------------------------
+mutable struct NVIDIA_ILU0
+    h::Ptr{Cvoid}
+    n::Int
+end
+mutable struct NVIDIA_IC0
+    h::Ptr{Cvoid}
+    n::Int
+end
+const DevicePrec = Union{NVIDIA_ILU0,NVIDIA_IC0}
+
+function _prec(fn::Symbol, A, nrhs, factor_type)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    d = Ref(desc(A))
+    fd = factor_type === Float32 ? 1 : 0
+    check(ccall((fn, libbpf), Cint, (Ptr{Cvoid}, Ref{CsrDesc}, Cint, Cint, Ref{Ptr{Cvoid}}),
+                ctx(), d, nrhs, fd, r))
+    return r[]
+end
+
+function ilu0(A::CuSparseMatrixCSR{Float64,Cint}, nrhs::Int; factor_type=Float64)
+    P = NVIDIA_ILU0(_prec(:bpf_ilu0_create, A, nrhs, factor_type), size(A, 1))
+    finalizer(p -> ccall((:bpf_prec_destroy, libbpf), Cint, (Ptr{Cvoid},), p.h), P)
+    return P
+end
+
+function ic0(A::CuSparseMatrixCSR{Float64,Cint}, nrhs::Int; factor_type=Float64)
+    P = NVIDIA_IC0(_prec(:bpf_ic0_create, A, nrhs, factor_type), size(A, 1))
+    finalizer(p -> ccall((:bpf_prec_destroy, libbpf), Cint, (Ptr{Cvoid},), p.h), P)
+    return P
+end
+
+function ldiv!(y::CuVecOrMat{Float64}, P::DevicePrec, x::CuVecOrMat{Float64})
+    p = size(x, 2)
+    check(ccall((:bpf_prec_apply, libbpf), Cint,
+                (Ptr{Cvoid}, Cint, CuPtr{Cdouble}, Cint, CuPtr{Cdouble}, Cint),
+                P.h, p, pointer(x), stride(x, 2), pointer(y), stride(y, 2)))
+    return y
+end
+
+# ---- block-GMRES (src/block_gmres.jl:127-154) -----------------------------------------
+_handle(::typeof(I)) = C_NULL
+_handle(P::DevicePrec) = P.h
+
+function block_gmres(A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64},
+                     X0::Union{Nothing,CuMatrix{Float64}}=nothing; memory::Int=20, M=I, N=I,
+                     ldiv::Bool=false, restart::Bool=false, reorthogonalization::Bool=false,
+                     atol::Float64=√eps(Float64), rtol::Float64=√eps(Float64), itmax::Int=0,
+                     timemax::Float64=Inf, verbose::Int=0, history::Bool=false)
+    n, p = size(B)
+    size(A, 1) == size(A, 2) || error("System must be square")
+    size(A, 1) == n || error("Inconsistent problem size")
+    X = CuMatrix{Float64}(undef, n, p)
+    cap = (itmax == 0 ? 2 * div(n, p) : itmax) + 2
+    res = zeros(Float64, cap)
+    opts = Ref(GmresOpts(memory, restart, reorthogonalization, ldiv, atol, rtol, itmax,
+                         isfinite(timemax) ? timemax : 0.0, verbose, history))
+    st = Ref(CStats(0, 0, 0, 0.0, 0, cap, pointer(res), 0))
+    x0p = X0 === nothing ? CU_NULL : pointer(X0)
+    GC.@preserve res begin
+        check(ccall((:bpf_block_gmres, libbpf), Cint,
+                    (Ptr{Cvoid}, Ref{CsrDesc}, Cint, CuPtr{Cdouble}, Cint, CuPtr{Cdouble}, Cint,
+                     CuPtr{Cdouble}, Cint, Ptr{Cvoid}, Ptr{Cvoid}, Ref{GmresOpts}, Ref{CStats}),
+                    ctx(), Ref(desc(A)), p, pointer(B), stride(B, 2), pointer(X), stride(X, 2),
+                    x0p, n, _handle(M), _handle(N), opts, st))
+    end
+    s = st[]
+    stats = BlockGMRESStats{Float64}(s.niter, s.solved != 0,
+                                     history ? res[1:min(s.n_residuals, cap)] : Float64[],
+                                     s.timer, status_string(s.status))
+    return X, stats
+end
+
+# ---- block-BiCGSTAB (src/block_bicgstab.jl:182-299) -----------------------------------
+function block_bicgstab(A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64};
+                        C::Union{Nothing,CuMatrix{Float64}}=nothing, N=I,
+                        atol::Float64=√eps(Float64), rtol::Float64=√eps(Float64), itmax::Int=0,
+                        timemax::Float64=Inf, verbose::Int=0, history::Bool=false)
+    n, p = size(B)
+    size(A, 1) == size(A, 2) || error("System must be square")
+    size(A, 1) == n || error("Inconsistent problem size")
+    X = CuMatrix{Float64}(undef, n, p)
+    cap = (itmax == 0 ? 2n : itmax) + 2
+    res = zeros(Float64, cap)
+    opts = Ref(BicgstabOpts(atol, rtol, itmax, isfinite(timemax) ? timemax : 0.0, verbose, history))
+    st = Ref(CStats(0, 0, 0, 0.0, 0, cap, pointer(res), 0))
+    cp = C === nothing ? CU_NULL : pointer(C)
+    GC.@preserve res begin
+        check(ccall((:bpf_block_bicgstab, libbpf), Cint,
+                    (Ptr{Cvoid}, Ref{CsrDesc}, Cint, CuPtr{Cdouble}, Cint, CuPtr{Cdouble}, Cint,
+                     CuPtr{Cdouble}, Cint, Ptr{Cvoid}, Ref{BicgstabOpts}, Ref{CStats}),
+                    ctx(), Ref(desc(A)), p, pointer(B), stride(B, 2), pointer(X), stride(X, 2),
+                    cp, n, _handle(N), opts, st))
+    end
+    s = st[]
+    return X, SimpleStats{Float64}(s.niter, s.solved != 0,
+                                   history ? res[1:min(s.n_residuals, cap)] : Float64[],
+                                   s.timer, status_string(s.status))
+end
+
+# ---- CUSOLVERRF (src/cusolverRF.jl) ----------------------------------------------------
+module CUSOLVERRF
+using CUDA, CUDA.CUSPARSE, LinearAlgebra
+import ..BlockPowerFlowB200: libbpf, ctx, check, desc, CsrDesc
+
+const ORDER = Dict(:AMD => 0, :MDQ => 1, :METIS => 2, :RCM => 3)
+
+abstract type CusolverFactorization{T} <: LinearAlgebra.Factorization{T} end
+mutable struct CusolverRfLU{T} <: CusolverFactorization{T}
+    h::Ptr{Cvoid}
+    n::Int
+end
+mutable struct CusolverRfLUBatch{T} <: CusolverFactorization{T}
+    h::Ptr{Cvoid}
+    batchsize::Int
+    n::Int
+end
+
+function _analyze(A, ordering, tol, fast_mode, batch)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:bpf_rf_analyze, libbpf), Cint,
+                (Ptr{Cvoid}, Ref{CsrDesc}, Cint, Cdouble, Cint, Cint, Ref{Ptr{Cvoid}}),
+                ctx(), Ref(desc(A)), ORDER[ordering], tol, fast_mode, batch, r))
+    return r[]
+end
+
+function CusolverRfLU(A::CuSparseMatrixCSR{T}; nrhs=1, ordering=:AMD, tol=1e-8, fast_mode=true) where T
+    @assert size(A, 1) == size(A, 2)
+    return CusolverRfLU{T}(_analyze(A, ordering, tol, fast_mode, 1), size(A, 1))
+end
+
+function CusolverRfLUBatch(A::CuSparseMatrixCSR{T}, batchsize::Int; ordering=:AMD, tol=1e-8,
+                           fast_mode=false) where T
+    @assert size(A, 1) == size(A, 2)
+    batchsize == 1 && error("Please specify a number of batch greater than 1 for `CuSolverRfLUBatch`")
+    return CusolverRfLUBatch{T}(_analyze(A, ordering, tol, fast_mode, batchsize), batchsize, size(A, 1))
+end
+
+update!(rflu::CusolverFactorization, A::CuSparseMatrixCSR) =
+    check(ccall((:bpf_rf_refactor, libbpf), Cint, (Ptr{Cvoid}, CuPtr{Cdouble}), rflu.h, pointer(A.nzVal)))
+
+rf_batch_refactor!(rflu::CusolverRfLUBatch, Anzval::CuMatrix{Float64}) =
+    check(ccall((:bpf_rf_refactor_batch, libbpf), Cint, (Ptr{Cvoid}, CuPtr{Cdouble}, Cint),
+                rflu.h, pointer(Anzval), stride(Anzval, 2)))
+
+function LinearAlgebra.ldiv!(rflu::CusolverFactorization, X::CuVecOrMat{Float64})
+    check(ccall((:bpf_rf_solve, libbpf), Cint, (Ptr{Cvoid}, Cint, CuPtr{Cdouble}, Cint),
+                rflu.h, size(X, 2), pointer(X), stride(X, 2)))
+    return X
+end
+function LinearAlgebra.ldiv!(x::CuVecOrMat{Float64}, rflu::CusolverFactorization, b::CuVecOrMat{Float64})
+    copyto!(x, b)
+    return ldiv!(rflu, x)
+end
+function solve!(x::Vector{<:CuVector{Float64}}, rflu::CusolverRfLUBatch, b::Vector{<:CuVector{Float64}})
+    X = reduce(hcat, b)
+    ldiv!(rflu, X)
+    for i in eachindex(x)
+        copyto!(x[i], view(X, :, i))
+    end
+end
+
+LinearAlgebra.lu(A::CuSparseMatrixCSR; options...) = CusolverRfLU(A; options...)
+LinearAlgebra.lu!(rflu::CusolverFactorization, A::CuSparseMatrixCSR) = update!(rflu, A)
+cudestroy!(rflu::CusolverFactorization) =
+    (rflu.h != C_NULL && ccall((:bpf_rf_destroy, libbpf), Cint, (Ptr{Cvoid},), rflu.h); rflu.h = C_NULL)
+end # module CUSOLVERRF
+
+end # module

@@ -127,6 +127,26 @@ BPF_API const char *bpf_solve_status_string(int status);
 /* Number of kernels this library launched on the context (a running counter). */
 BPF_API long long bpf_ctx_kernel_launches(const bpf_ctx *ctx);
 
+/* Per-kernel-class device timing (CUDA events recorded around each launch on the context's
+ * stream).  No counterpart in the reference: it stands in for the CUDA.@time / @time
+ * measurements of test/*.jl and is what the benchmark uses to put a launch-averaged kernel
+ * duration next to its roofline.  bpf_ctx_set_timing(ctx, 1) clears and starts recording. */
+typedef enum {
+    BPF_KC_SPMM = 0,    /* CSR SpMM                                   */
+    BPF_KC_TRSV = 1,    /* preconditioner / RF triangular solves      */
+    BPF_KC_FACTOR = 2,  /* ILU0 / IC0 / RF numeric factorization      */
+    BPF_KC_GRAM = 3,    /* block Gram products (split over rows)      */
+    BPF_KC_TSMM = 4,    /* tall x small block products                */
+    BPF_KC_SMALL = 5,   /* one-CTA p x p kernels (Cholesky, Hessenberg) */
+    BPF_KC_COUNT = 6
+} bpf_kernel_class;
+BPF_API bpf_status bpf_ctx_set_timing(bpf_ctx *ctx, int on);
+/* Totals since bpf_ctx_set_timing(ctx, 1): device milliseconds, launches, and the launches'
+ * algorithmic DRAM bytes and flops (the roofline numerators; each kernel's formula is stated
+ * beside it in the sources).  Any output pointer may be NULL. */
+BPF_API bpf_status bpf_ctx_kernel_time(bpf_ctx *ctx, int kernel_class, double *total_ms,
+                                       long long *launches, double *bytes, double *flops);
+
 /* ---- sparse x dense block -------------------------------------------------------------- */
 /* Y = alpha*A*X + beta*Y: mul!(W, A, P) of src/block_gmres.jl:299 (CSR SpMM). */
 BPF_API bpf_status bpf_spmm(bpf_ctx *ctx, const bpf_csr_desc *A, int p, double alpha,
