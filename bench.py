@@ -182,6 +182,20 @@ def kernel_only(name, reps):
 
     import blockpowerflow_b200 as bpf
 
+    if name == "gmres":
+        # 24 iterations of the benchmark's solve (9,000-bus grid, 64 RHS): every kernel of the
+        # block-GMRES iteration, for a launch list
+        J, B = make_workload(0)
+        A = bpf.CuSparseMatrixCSR.from_scipy(J)
+        Bd = bpf.colmajor(torch.as_tensor(B, device="cuda"))
+        N = bpf.ilu0(A, P_RHS)
+        for _ in range(reps):
+            X, st = bpf.block_gmres(A, Bd, N=N, ldiv=True, restart=False, memory=ITMAX, atol=0.0,
+                                    rtol=RTOL, itmax=24)
+        torch.cuda.synchronize()
+        print(json.dumps({"kernel_only": name, "n": J.shape[0], "p": P_RHS, "reps": reps,
+                          "iterations": st.niter}))
+        return
     J = bpf.grid.preset_jacobian("case70k", 0)
     n = J.shape[0]
     p = 128
@@ -205,7 +219,7 @@ def kernel_only(name, reps):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel-only", choices=["trsv", "spmm", "factor", "gram"], default=None,
+    ap.add_argument("--kernel-only", choices=["trsv", "spmm", "factor", "gram", "gmres"], default=None,
                     help="launch one kernel a few times on a 135k-unknown case (for ncu)")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--gpus", type=int, default=1)

@@ -193,6 +193,7 @@ bpf_status bpf_ctx_create(bpf_ctx **out, void *stream) {
     *out = nullptr;
     bpf_ctx *ctx = new bpf_ctx();
     ctx->stream = (cudaStream_t)stream;
+    if (const char *env = getenv("BPF_FP64_MMA")) ctx->fp64_mma = atoi(env) != 0;
     cudaError_t e = cudaGetDevice(&ctx->device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
     if (e == cudaSuccess)

@@ -66,6 +66,9 @@ struct bpf_ctx {
     int max_smem_optin = 0;
     std::string last_error;
     long long launches = 0;
+    // FP64 block products on the tensor pipe (DMMA) instead of FMA; BPF_FP64_MMA=0 turns it
+    // off (used to compare the two paths).
+    bool fp64_mma = true;
     // per-kernel-class event timing (bpf_ctx_set_timing)
     bool timing = false;
     std::vector<cudaEvent_t> event_pool;

@@ -16,6 +16,7 @@
 
 #include "bpf_internal.cuh"
 #include "dense.cuh"
+#include "small.cuh"
 
 namespace bpf {
 
@@ -106,6 +107,12 @@ __global__ void gram_reduce_kernel(int total, int nchunks, const double *__restr
     }
 }
 
+template <int GT>
+__global__ void gram_dmma_kernel(int n, int p, int nb, const double *__restrict__ A,
+                                 size_t strideA, const double *__restrict__ B,
+                                 double *__restrict__ partial, int rows_per_chunk,
+                                 const SolveState *st, const int *gate, const int *gate2);
+
 bpf_status gram(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t strideA,
                 const double *B, double *Out, double alpha, bool accumulate,
                 const SolveState *st, const int *qr_gate, double *Out2, const int *gate2) {
@@ -123,7 +130,17 @@ bpf_status gram(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
     if (!partial) return s;
     dim3 grid(nchunks, nb, tiles);
     KScope ks(ctx, BPF_KC_GRAM, 8.0 * n * p * (nb + (A == B ? 0 : 1)), 2.0 * n * p * (double)p * nb);
-    if (GT == 16)
+    if (ctx->fp64_mma) {
+        if (GT == 16)
+            gram_dmma_kernel<16><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
+                                                                 rows_per_chunk, st, qr_gate, gate2);
+        else if (GT == 32)
+            gram_dmma_kernel<32><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
+                                                                 rows_per_chunk, st, qr_gate, gate2);
+        else
+            gram_dmma_kernel<64><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
+                                                                 rows_per_chunk, st, qr_gate, gate2);
+    } else if (GT == 16)
         gram_partial_kernel<16><<<grid, 256, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
                                                                 rows_per_chunk, st, qr_gate, gate2);
     else if (GT == 32)
@@ -139,6 +156,151 @@ bpf_status gram(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
                                                          accumulate ? 1 : 0, Out2, st, qr_gate, gate2);
     BPF_LAUNCHED(ctx);
     return BPF_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------------------
+// FP64 tensor-core (DMMA, mma.sync m8n8k4 f64) versions of gram and tsmm.
+// Fragment layout of mma.sync.aligned.m8n8k4.row.col.f64: lane = 4 g + t, A[g][t],
+// B[t][g], C[g][2t], C[g][2t+1].  Shared-memory rows are padded to a stride = 4 (mod 16)
+// doubles so both half-warps read 16 distinct 8-byte banks.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void dmma884(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// Out tile GT x GT of A_j^T B over a chunk of rows; 4 warps in a 2 x 2 layout.
+template <int GT>
+__global__ void __launch_bounds__(128)
+gram_dmma_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
+                 const double *__restrict__ B, double *__restrict__ partial, int rows_per_chunk,
+                 const SolveState *st, const int *gate, const int *gate2) {
+    if (gate_off(st, gate, gate2)) return;
+    constexpr int RS = 32, S = GT + 4, WT = GT / 2, MT = WT / 8;
+    __shared__ double As[RS * S];
+    __shared__ double Bs[RS * S];
+    const int chunk = blockIdx.x, j = blockIdx.y;
+    const int ntile = (p + GT - 1) / GT;
+    const int a0 = (blockIdx.z / ntile) * GT, b0 = (blockIdx.z % ntile) * GT;
+    const int r_begin = chunk * rows_per_chunk;
+    const int r_end = min(n, r_begin + rows_per_chunk);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t4 = lane & 3;
+    const double *Aj = A + (size_t)j * strideA;
+    double acc[MT][MT][2];
+#pragma unroll
+    for (int mi = 0; mi < MT; mi++)
+#pragma unroll
+        for (int ni = 0; ni < MT; ni++) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+    for (int r0 = r_begin; r0 < r_end; r0 += RS) {
+        for (int e = tid; e < RS * GT; e += 128) {
+            const int rr = e / GT, cc = e % GT, r = r0 + rr;
+            const bool rok = r < r_end;
+            As[rr * S + cc] = (rok && a0 + cc < p) ? __ldg(Aj + (size_t)r * p + a0 + cc) : 0.0;
+            Bs[rr * S + cc] = (rok && b0 + cc < p) ? __ldg(B + (size_t)r * p + b0 + cc) : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < RS / 4; ks++) {
+            const int k = ks * 4 + t4;
+            double a[MT], b[MT];
+#pragma unroll
+            for (int mi = 0; mi < MT; mi++) a[mi] = As[k * S + wm * WT + mi * 8 + g];
+#pragma unroll
+            for (int ni = 0; ni < MT; ni++) b[ni] = Bs[k * S + wn * WT + ni * 8 + g];
+#pragma unroll
+            for (int mi = 0; mi < MT; mi++)
+#pragma unroll
+                for (int ni = 0; ni < MT; ni++) dmma884(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+        }
+        __syncthreads();
+    }
+    double *out = partial + ((size_t)chunk * nb + j) * p * p;
+#pragma unroll
+    for (int mi = 0; mi < MT; mi++) {
+        const int row = a0 + wm * WT + mi * 8 + g;
+        if (row >= p) continue;
+#pragma unroll
+        for (int ni = 0; ni < MT; ni++) {
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                const int col = b0 + wn * WT + ni * 8 + 2 * t4 + i;
+                if (col < p) out[(size_t)row * p + col] = acc[mi][ni][i];
+            }
+        }
+    }
+}
+
+// Out rows r0..r0+63, columns b0..b0+GT-1 of beta*C + alpha*sum_j A_j S_j; 4 warps 2 x 2.
+template <int GT>
+__global__ void __launch_bounds__(128)
+tsmm_dmma_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
+                 const double *__restrict__ S, size_t strideS, double alpha, const double *Cin,
+                 double beta, double *Out, const SolveState *st, const int *nb_dev,
+                 const int *gate, const int *gate2) {
+    if (gate_off(st, gate, gate2)) return;
+    constexpr int KC = 32, SA = KC + 4, SB = GT + 4, WN = GT / 2, MTN = WN / 8;
+    __shared__ double As[64 * SA];
+    __shared__ double Bs[KC * SB];
+    const int r0 = blockIdx.x * 64;
+    const int b0 = blockIdx.y * GT;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t4 = lane & 3;
+    int nbl = nb;
+    if (nb_dev) nbl = min(nb, *nb_dev);
+    double acc[4][MTN][2];
+#pragma unroll
+    for (int mi = 0; mi < 4; mi++)
+#pragma unroll
+        for (int ni = 0; ni < MTN; ni++) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+    for (int j = 0; j < nbl; j++) {
+        const double *Aj = A + (size_t)j * strideA;
+        const double *Sj = S + (size_t)j * strideS;
+        for (int k0 = 0; k0 < p; k0 += KC) {
+            for (int e = tid; e < 64 * KC; e += 128) {
+                const int rr = e / KC, kk = e % KC;
+                const int r = r0 + rr, c = k0 + kk;
+                As[rr * SA + kk] = (r < n && c < p) ? __ldg(Aj + (size_t)r * p + c) : 0.0;
+            }
+            for (int e = tid; e < KC * GT; e += 128) {
+                const int kk = e / GT, cc = e % GT;
+                const int a = k0 + kk, b = b0 + cc;
+                Bs[kk * SB + cc] = (a < p && b < p) ? __ldg(Sj + (size_t)a * p + b) : 0.0;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int ks = 0; ks < KC / 4; ks++) {
+                const int k = ks * 4 + t4;
+                double a[4], b[MTN];
+#pragma unroll
+                for (int mi = 0; mi < 4; mi++) a[mi] = As[(wm * 32 + mi * 8 + g) * SA + k];
+#pragma unroll
+                for (int ni = 0; ni < MTN; ni++) b[ni] = Bs[k * SB + wn * WN + ni * 8 + g];
+#pragma unroll
+                for (int mi = 0; mi < 4; mi++)
+#pragma unroll
+                    for (int ni = 0; ni < MTN; ni++) dmma884(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+            }
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int mi = 0; mi < 4; mi++) {
+        const int r = r0 + wm * 32 + mi * 8 + g;
+        if (r >= n) continue;
+#pragma unroll
+        for (int ni = 0; ni < MTN; ni++) {
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                const int b = b0 + wn * WN + ni * 8 + 2 * t4 + i;
+                if (b >= p) continue;
+                double v = alpha * acc[mi][ni][i];
+                if (Cin && beta != 0.0) v += beta * Cin[(size_t)r * p + b];
+                Out[(size_t)r * p + b] = v;
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -219,7 +381,17 @@ bpf_status tsmm(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
     dim3 grid(ceil_div(n, kTsmmRows), ceil_div(p, GT));
     KScope ks(ctx, BPF_KC_TSMM, 8.0 * n * p * (nb + 1 + ((Cin && beta != 0.0) ? 1 : 0)),
               2.0 * n * p * (double)p * nb);
-    if (GT == 16)
+    if (ctx->fp64_mma) {
+        if (GT == 16)
+            tsmm_dmma_kernel<16><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, S, strideS, alpha,
+                                                                 Cin, beta, Out, st, nb_dev, qr_gate, gate2);
+        else if (GT == 32)
+            tsmm_dmma_kernel<32><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, S, strideS, alpha,
+                                                                 Cin, beta, Out, st, nb_dev, qr_gate, gate2);
+        else
+            tsmm_dmma_kernel<64><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, S, strideS, alpha,
+                                                                 Cin, beta, Out, st, nb_dev, qr_gate, gate2);
+    } else if (GT == 16)
         tsmm_kernel<16><<<grid, 256, 0, ctx->stream>>>(n, p, nb, A, strideA, S, strideS, alpha, Cin,
                                                         beta, Out, st, nb_dev, qr_gate, gate2);
     else if (GT == 32)
@@ -232,125 +404,6 @@ bpf_status tsmm(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
     return BPF_SUCCESS;
 }
 
-// ---------------------------------------------------------------------------------------
-// Cholesky of the Gram matrix (one CTA): G = R^T R, R upper; Rinv = R^{-1};
-// Racc <- R * Racc (or R when first).  pass 0 may shift G (Fukaya et al., shifted CholeskyQR:
-// s = 11 (n p + p (p+1)) u ||G||, ||G|| bounded by trace(G)) when a pivot falls below
-// 1e-13 of the column's original norm; it then sets st->qr_shift so the third pass runs.
-// ---------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024)
-chol_kernel(int n, int p, const double *__restrict__ G, double *__restrict__ Rinv,
-            double *__restrict__ Racc, double *__restrict__ Rtmp, int pass, SolveState *st,
-            const int *gate, const int *gate2, int *shift_flag, int *reorth_flag, DevStatus *ds) {
-    if (st && !st->active) return;
-    if (gate && *gate == 0) return;
-    if (gate2 && *gate2 == 0) return;
-    extern __shared__ double g[];            // p*p
-    __shared__ int s_fail;
-    __shared__ double s_shift;
-    __shared__ double s_minratio;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int pp = p * p;
-    if (pass == 0 && tid == 0 && shift_flag) *shift_flag = 0;
-    if (tid == 0) s_minratio = 1.0;
-    double trace = 0.0;
-    for (int i = 0; i < p; i++) trace += G[i * p + i];
-    for (int attempt = 0; attempt < 2; attempt++) {
-        if (tid == 0) {
-            s_fail = 0;
-            s_shift = attempt == 0 ? 0.0
-                                   : 11.0 * ((double)n * p + (double)p * (p + 1)) * 1.1102230246251565e-16 * trace;
-        }
-        __syncthreads();
-        for (int e = tid; e < pp; e += nt) g[e] = G[e] + ((e / p == e % p) ? s_shift : 0.0);
-        __syncthreads();
-        for (int j = 0; j < p; j++) {
-            if (tid == 0) {
-                double d = g[j * p + j];
-                double ref = G[j * p + j] + s_shift;
-                if (attempt == 0) s_minratio = fmin(s_minratio, (ref > 0.0) ? d / ref : 0.0);
-                if (!(d > 1e-13 * ref) || !(d > 0.0)) {
-                    s_fail = 1;
-                } else {
-                    g[j * p + j] = sqrt(d);
-                }
-            }
-            __syncthreads();
-            if (s_fail) break;
-            const double inv = 1.0 / g[j * p + j];
-            for (int c = j + 1 + tid; c < p; c += nt) g[j * p + c] *= inv;
-            __syncthreads();
-            const int m = p - j - 1;
-            for (int e = tid; e < m * m; e += nt) {
-                const int a = j + 1 + e / m, b = j + 1 + e % m;
-                if (b >= a) g[a * p + b] -= g[j * p + a] * g[j * p + b];
-            }
-            __syncthreads();
-        }
-        if (attempt == 0 && tid == 0 && pass == 0 && reorth_flag)
-            *reorth_flag = (s_fail || s_minratio < 1e-8) ? 1 : 0;
-        if (!s_fail) break;
-        if (attempt == 0 && shift_flag) {
-            if (tid == 0) *shift_flag = 1;
-        }
-        __syncthreads();
-    }
-    if (s_fail) {
-        if (tid == 0) {
-            if (st) st->qr_fail = 1;
-            if (ds && atomicCAS(&ds->err, 0, (int)DEV_CHOL_FAIL) == 0) ds->aux = pass;
-        }
-        return;
-    }
-    // zero the strict lower triangle so g holds R
-    for (int e = tid; e < pp; e += nt)
-        if (e / p > e % p) g[e] = 0.0;
-    __syncthreads();
-    // Rinv: warp w solves R x = e_c for columns c = w, w+nwarps, ...
-    const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
-    for (int c = warp; c < p; c += nwarps) {
-        double b[4];
-#pragma unroll
-        for (int t = 0; t < 4; t++) {
-            const int r = lane + 32 * t;
-            b[t] = (r == c) ? 1.0 : 0.0;
-        }
-        for (int k = c; k >= 0; k--) {
-            const int owner = k & 31, slot = k >> 5;
-            double bk = 0.0;
-#pragma unroll
-            for (int t = 0; t < 4; t++)
-                if (t == slot) bk = b[t];
-            bk = __shfl_sync(0xffffffffu, bk, owner);
-            const double xk = bk / g[k * p + k];
-#pragma unroll
-            for (int t = 0; t < 4; t++) {
-                const int r = lane + 32 * t;
-                if (r == k) b[t] = xk;
-                else if (r < k) b[t] -= g[r * p + k] * xk;
-            }
-        }
-#pragma unroll
-        for (int t = 0; t < 4; t++) {
-            const int r = lane + 32 * t;
-            if (r < p) Rinv[r * p + c] = (r <= c) ? b[t] : 0.0;
-        }
-    }
-    // Racc <- R * Racc (pass > 0) or R (pass 0)
-    if (pass == 0) {
-        for (int e = tid; e < pp; e += nt) Racc[e] = g[e];
-    } else {
-        for (int e = tid; e < pp; e += nt) {
-            const int a = e / p, b = e % p;
-            double s = 0.0;
-            for (int c = a; c <= b; c++) s += g[a * p + c] * Racc[c * p + b];
-            Rtmp[e] = (b >= a) ? s : 0.0;
-        }
-        __syncthreads();
-        for (int e = tid; e < pp; e += nt) Racc[e] = Rtmp[e];
-    }
-}
-
 __global__ void gated_copy_kernel(size_t len, const double *__restrict__ src,
                                   double *__restrict__ dst, const SolveState *st, const int *gate,
                                   const int *gate2) {
@@ -358,22 +411,6 @@ __global__ void gated_copy_kernel(size_t len, const double *__restrict__ src,
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < len;
          e += (size_t)gridDim.x * blockDim.x)
         dst[e] = src[e];
-}
-
-static bpf_status launch_chol(bpf_ctx *ctx, int n, int p, const double *G, double *Rinv,
-                              double *Racc, double *Rtmp, int pass, SolveState *st,
-                              const int *gate, const int *gate2, int *shift_flag,
-                              int *reorth_flag) {
-    size_t smem = sizeof(double) * p * p;
-    if (smem > 48 * 1024) {
-        BPF_CUDA(ctx, cudaFuncSetAttribute(chol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem));
-    }
-    KScope ks(ctx, BPF_KC_SMALL);
-    chol_kernel<<<1, 1024, smem, ctx->stream>>>(n, p, G, Rinv, Racc, Rtmp, pass, st, gate, gate2,
-                                                shift_flag, reorth_flag, ctx->dstat);
-    BPF_LAUNCHED(ctx);
-    return BPF_SUCCESS;
 }
 
 bpf_status cholqr(bpf_ctx *ctx, int n, int p, const double *W, double *Q, double *R,

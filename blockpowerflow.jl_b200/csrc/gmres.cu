@@ -29,6 +29,7 @@
 #include "bpf_internal.cuh"
 #include "dense.cuh"
 #include "prec.cuh"
+#include "small.cuh"
 
 namespace bpf {
 
@@ -55,205 +56,6 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
-}
-
-// ---------------------------------------------------------------------------------------
-// Apply the stored block reflectors Omega_0..Omega_{j-1} to block column j of the
-// Hessenberg matrix (packed R blocks).  One CTA per column b of the block column; only the
-// two p-segments a reflector touches are held in shared memory.
-// HY layout per block column i: Y_i (2p x p, explicit: 0 above, 1 on the diagonal) then
-// T_i (p x p upper), so Omega_i^T = I - Y_i T_i^T Y_i^T.
-// ---------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256)
-hess_apply_kernel(int p, int k, double *__restrict__ Rblk, const double *__restrict__ HY,
-                  const SolveState *st) {
-    if (!st->active) return;
-    const int j = k - 1;
-    if (j <= 0) return;
-    const int b = blockIdx.x;
-    extern __shared__ double sm[];
-    double *seg = sm;            // 2p
-    double *w = sm + 2 * p;      // p
-    double *w2 = w + p;          // p
-    const size_t pp = (size_t)p * p;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int a = threadIdx.x; a < p; a += blockDim.x) seg[a] = Rblk[rpos(0, j) * pp + (size_t)a * p + b];
-    for (int i = 0; i < j; i++) {
-        for (int a = threadIdx.x; a < p; a += blockDim.x)
-            seg[p + a] = Rblk[rpos(i + 1, j) * pp + (size_t)a * p + b];
-        __syncthreads();
-        const double *Y = HY + (size_t)i * 3 * pp;
-        const double *T = Y + 2 * pp;
-        for (int c = warp; c < p; c += nw) {
-            double s = 0.0;
-            for (int r = c + lane; r < 2 * p; r += 32) s += Y[(size_t)r * p + c] * seg[r];
-            s = warp_sum(s);
-            if (lane == 0) w[c] = s;
-        }
-        __syncthreads();
-        for (int c = threadIdx.x; c < p; c += blockDim.x) {
-            double s = 0.0;
-            for (int cp = 0; cp <= c; cp++) s += T[(size_t)cp * p + c] * w[cp];
-            w2[c] = s;
-        }
-        __syncthreads();
-        for (int r = threadIdx.x; r < 2 * p; r += blockDim.x) {
-            const int cmax = min(r, p - 1);
-            double s = 0.0;
-            for (int c = 0; c <= cmax; c++) s += Y[(size_t)r * p + c] * w2[c];
-            seg[r] -= s;
-        }
-        __syncthreads();
-        for (int a = threadIdx.x; a < p; a += blockDim.x) {
-            Rblk[rpos(i, j) * pp + (size_t)a * p + b] = seg[a];
-            seg[a] = seg[p + a];
-        }
-        __syncthreads();
-    }
-    for (int a = threadIdx.x; a < p; a += blockDim.x) Rblk[rpos(j, j) * pp + (size_t)a * p + b] = seg[a];
-}
-
-// ---------------------------------------------------------------------------------------
-// Factor [R_jj; C] (2p x p) with Householder reflections (LAPACK dlarfg conventions), build
-// the compact-WY T factor, apply Omega_j^T to [Z_j; 0], and run the stopping test.
-// One CTA; operands live in global memory (L1-resident), ordered by __syncthreads.
-// ---------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024)
-hess_factor_kernel(int p, int k, double *__restrict__ Rblk, double *__restrict__ HY,
-                   double *__restrict__ tau_all, double *__restrict__ Z,
-                   const double *__restrict__ Cm, SolveState *st, double *__restrict__ hist,
-                   double *__restrict__ scr) {
-    if (!st->active) return;
-    __shared__ double red[32];
-    __shared__ double s_scale;
-    const int j = k - 1;
-    const size_t pp = (size_t)p * p;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-    double *F = HY + (size_t)j * 3 * pp;
-    double *T = F + 2 * pp;
-    double *tau = tau_all;  // reflector scalars of the current block (T keeps them too)
-    double *Rjj = Rblk + rpos(j, j) * pp;
-    double *Zj = Z + (size_t)j * pp;
-    double *Zn = Z + (size_t)(j + 1) * pp;
-    double *YtY = scr, *W1 = scr + pp, *W2 = scr + 2 * pp;
-    const int m = 2 * p;
-    for (size_t e = tid; e < pp; e += nt) {
-        F[e] = Rjj[e];
-        F[pp + e] = Cm[e];
-    }
-    __syncthreads();
-    for (int c = 0; c < p; c++) {
-        double s = 0.0;
-        for (int r = c + 1 + tid; r < m; r += nt) {
-            const double v = F[(size_t)r * p + c];
-            s += v * v;
-        }
-        s = block_sum(s, red);
-        if (tid == 0) {
-            const double alpha = F[(size_t)c * p + c];
-            const double xn = sqrt(s);
-            if (xn == 0.0) {
-                tau[c] = 0.0;
-                s_scale = 0.0;
-            } else {
-                const double beta = -copysign(hypot(alpha, xn), alpha);
-                tau[c] = (beta - alpha) / beta;
-                s_scale = 1.0 / (alpha - beta);
-                F[(size_t)c * p + c] = beta;
-            }
-        }
-        __syncthreads();
-        const double t = tau[c];
-        if (t != 0.0) {
-            const double sc = s_scale;
-            for (int r = c + 1 + tid; r < m; r += nt) F[(size_t)r * p + c] *= sc;
-            __syncthreads();
-            for (int c2 = c + 1 + warp; c2 < p; c2 += nw) {
-                double wv = 0.0;
-                for (int r = c + 1 + lane; r < m; r += 32) wv += F[(size_t)r * p + c] * F[(size_t)r * p + c2];
-                wv = warp_sum(wv) + F[(size_t)c * p + c2];
-                wv *= t;
-                if (lane == 0) F[(size_t)c * p + c2] -= wv;
-                for (int r = c + 1 + lane; r < m; r += 32) F[(size_t)r * p + c2] -= wv * F[(size_t)r * p + c];
-            }
-        }
-        __syncthreads();
-    }
-    // R_jj <- upper triangle; F <- explicit Y
-    for (size_t e = tid; e < pp; e += nt) {
-        const int a = (int)(e / p), b = (int)(e % p);
-        Rjj[e] = (b >= a) ? F[e] : 0.0;
-    }
-    __syncthreads();
-    for (size_t e = tid; e < 2 * pp; e += nt) {
-        const int r = (int)(e / p), c = (int)(e % p);
-        if (r < c) F[e] = 0.0;
-        else if (r == c) F[e] = 1.0;
-    }
-    for (size_t e = tid; e < pp; e += nt) T[e] = 0.0;
-    __syncthreads();
-    // YtY[a][c] = y_a . y_c for a < c (rows r >= c)
-    for (size_t e = tid; e < pp; e += nt) {
-        const int a = (int)(e / p), c = (int)(e % p);
-        if (a < c) {
-            double s = 0.0;
-            for (int r = c; r < m; r++) s += F[(size_t)r * p + a] * F[(size_t)r * p + c];
-            YtY[e] = s;
-        }
-    }
-    __syncthreads();
-    // T(0:c, c) = -tau_c T(0:c, 0:c) YtY(0:c, c); T(c, c) = tau_c   (dlarft, forward)
-    for (int c = 0; c < p; c++) {
-        const double tc = tau[c];
-        for (int a = tid; a < c; a += nt) {
-            double s = 0.0;
-            for (int a2 = a; a2 < c; a2++) s += T[(size_t)a * p + a2] * YtY[(size_t)a2 * p + c];
-            T[(size_t)a * p + c] = -tc * s;
-        }
-        if (tid == 0) T[(size_t)c * p + c] = tc;
-        __syncthreads();
-    }
-    // [Z_j; Lambda] = Omega_j^T [Z_j; 0]
-    for (size_t e = tid; e < pp; e += nt) {
-        const int c = (int)(e / p), b = (int)(e % p);
-        double s = 0.0;
-        for (int r = c; r < p; r++) s += F[(size_t)r * p + c] * Zj[(size_t)r * p + b];
-        W1[e] = s;
-    }
-    __syncthreads();
-    for (size_t e = tid; e < pp; e += nt) {
-        const int c = (int)(e / p), b = (int)(e % p);
-        double s = 0.0;
-        for (int c2 = 0; c2 <= c; c2++) s += T[(size_t)c2 * p + c] * W1[(size_t)c2 * p + b];
-        W2[e] = s;
-    }
-    __syncthreads();
-    double ss = 0.0;
-    for (size_t e = tid; e < 2 * pp; e += nt) {
-        const int r = (int)(e / p), b = (int)(e % p);
-        const int cmax = min(r, p - 1);
-        double s = 0.0;
-        for (int c = 0; c <= cmax; c++) s += F[(size_t)r * p + c] * W2[(size_t)c * p + b];
-        if (r < p) {
-            Zj[e] -= s;
-        } else {
-            Zn[e - pp] = -s;
-            ss += s * s;
-        }
-    }
-    ss = block_sum(ss, red);
-    if (tid == 0) {
-        const double rn = sqrt(ss);
-        st->rnorm = rn;
-        if (st->nres < st->hist_cap) hist[st->nres] = rn;
-        st->nres++;
-        st->inner_iter = k;
-        st->solved = rn <= st->eps;
-        st->inner_tired = st->restart ? (k >= min(st->mem, st->inner_itmax)) : (k >= st->inner_itmax);
-        st->overtimed = (st->deadline_ns != 0ull && globaltimer_ns() > st->deadline_ns);
-        st->active = !(st->solved || st->inner_tired || st->overtimed);
-    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -532,12 +334,7 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
                     BPF_TRY(cholqr(ctx, n, p, Qk, Vn, C2, Tq, st, rg, &st->qr_shift2, nullptr));
                     BPF_TRY(reorth_fold(ctx, p, kk, Psi, Psi2buf, Cm, C2, Cm, fold_scr, st, rg));
                 }
-                KScope ks(ctx, BPF_KC_SMALL);
-                hess_apply_kernel<<<p, 256, sizeof(double) * 4 * p, ctx->stream>>>(p, kk, g.Rblk, g.HY, st);
-                BPF_LAUNCHED(ctx);
-                hess_factor_kernel<<<1, 1024, 0, ctx->stream>>>(p, kk, g.Rblk, g.HY, tau_cur, g.Z, Cm, st,
-                                                                 hist, scr);
-                BPF_LAUNCHED(ctx);
+                BPF_TRY(launch_hess(ctx, p, kk, g.Rblk, g.HY, tau_cur, g.Z, Cm, st, hist, scr));
             }
             k = kend;
             BPF_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(SolveState), cudaMemcpyDeviceToHost, ctx->stream));
