@@ -86,6 +86,7 @@ SIGNATURES = {
     "bpf_ic0_create": (_I, [_P, C.POINTER(CsrDesc), _I, _I, C.POINTER(_P)]),
     "bpf_prec_refactor": (_I, [_P, _P]),
     "bpf_prec_apply": (_I, [_P, _I, _P, _I, _P, _I]),
+    "bpf_prec_apply_noalloc": (_I, [_P, _I, _P, _I, _P, _I]),
     "bpf_prec_factor_values": (_I, [_P, _P]),
     "bpf_prec_levels": (_I, [_P, C.POINTER(_I), C.POINTER(_I)]),
     "bpf_prec_destroy": (_I, [_P]),

@@ -174,6 +174,15 @@ BPF_API bpf_status bpf_prec_refactor(bpf_prec *prec, const double *vals);
  * src/preconditioners_nvidia.jl:13-35,49-71.  Y may equal X. */
 BPF_API bpf_status bpf_prec_apply(bpf_prec *prec, int p, const double *X, int ldx, double *Y,
                                   int ldy);
+/* No counterpart in the reference.  The same Y = P \ X as bpf_prec_apply for callers that
+ * cannot allocate device memory once the preconditioner exists (code inside a stream capture,
+ * hosts whose device memory belongs to an external pool or a fixed start-up arena, loops that
+ * forbid allocation): its scratch is a static 8 MiB device array instead of a cudaMalloc'd
+ * workspace.  Limit: n * min(p, 256) <= 1,048,576 doubles, else BPF_ERR_NOT_SUPPORTED.  All calls
+ * on a device share the array (calls that overlap on the GPU race); the first call on a device
+ * looks its address up and should come before any stream capture. */
+BPF_API bpf_status bpf_prec_apply_noalloc(bpf_prec *prec, int p, const double *X, int ldx,
+                                          double *Y, int ldy);
 /* Copy the factor values (A's pattern, nnz doubles, device pointer) out: the P field of
  * NVIDIA_ILU0 / NVIDIA_IC0 (src/preconditioners_nvidia.jl:1-4,37-40). */
 BPF_API bpf_status bpf_prec_factor_values(const bpf_prec *prec, double *vals);
