@@ -54,6 +54,8 @@ enum Slot : int {
     WS_HY,            // Householder reflectors (2p x p) and T factors per block column
     WS_HSCR,          // scratch of the one-CTA small-matrix kernels
     WS_VEC,           // n x p working blocks of a solve
+    WS_Y,             // block back-substitution result Y
+    WS_ZB,            // flexible GMRES: preconditioned basis blocks
     WS_COUNT
 };
 

@@ -10,6 +10,8 @@
 //         Algorithmic bytes: 8*n*p*(nb + 1); flops 2*n*p*p*nb.
 //  tsmm : Out = beta*C + alpha*sum_j A_j S_j, one 64-row x 64-column tile per CTA.
 //         Algorithmic bytes: 8*n*p*(nb + 1 [+1 for C]); flops 2*n*p*p*nb.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -108,10 +110,10 @@ __global__ void gram_reduce_kernel(int total, int nchunks, const double *__restr
 }
 
 template <int GT>
-__global__ void gram_dmma_kernel(int n, int p, int nb, const double *__restrict__ A,
-                                 size_t strideA, const double *__restrict__ B,
-                                 double *__restrict__ partial, int rows_per_chunk,
-                                 const SolveState *st, const int *gate, const int *gate2);
+__global__ void gram_dmma_cl_kernel(int n, int p, int nb, const double *__restrict__ A,
+                                    size_t strideA, const double *__restrict__ B,
+                                    double *__restrict__ partial, int rows_per_chunk,
+                                    const SolveState *st, const int *gate, const int *gate2);
 
 bpf_status gram(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t strideA,
                 const double *B, double *Out, double alpha, bool accumulate,
@@ -125,21 +127,27 @@ bpf_status gram(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
     int rows_per_chunk = ceil_div(std::max(n, 1), nchunks);
     rows_per_chunk = ceil_div(rows_per_chunk, kGramRows) * kGramRows;
     nchunks = std::max(1, ceil_div(std::max(n, 1), rows_per_chunk));
+    // DMMA path: chunks in clusters of 8 (trailing chunks of the last cluster may be empty),
+    // one partial per cluster
+    const bool cl = ctx->fp64_mma;
+    const int nclusters = ceil_div(nchunks, 8);
+    const int grid_x = cl ? 8 * nclusters : nchunks;
+    const int nparts = cl ? nclusters : nchunks;
     bpf_status s;
-    double *partial = (double *)ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)nchunks * nb * p * p, &s);
+    double *partial = (double *)ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)nparts * nb * p * p, &s);
     if (!partial) return s;
-    dim3 grid(nchunks, nb, tiles);
+    dim3 grid(grid_x, nb, tiles);
     KScope ks(ctx, BPF_KC_GRAM, 8.0 * n * p * (nb + (A == B ? 0 : 1)), 2.0 * n * p * (double)p * nb);
-    if (ctx->fp64_mma) {
+    if (cl) {
         if (GT == 16)
-            gram_dmma_kernel<16><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
-                                                                 rows_per_chunk, st, qr_gate, gate2);
+            gram_dmma_cl_kernel<16><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
+                                                                    rows_per_chunk, st, qr_gate, gate2);
         else if (GT == 32)
-            gram_dmma_kernel<32><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
-                                                                 rows_per_chunk, st, qr_gate, gate2);
+            gram_dmma_cl_kernel<32><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
+                                                                    rows_per_chunk, st, qr_gate, gate2);
         else
-            gram_dmma_kernel<64><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
-                                                                 rows_per_chunk, st, qr_gate, gate2);
+            gram_dmma_cl_kernel<64><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
+                                                                    rows_per_chunk, st, qr_gate, gate2);
     } else if (GT == 16)
         gram_partial_kernel<16><<<grid, 256, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
                                                                 rows_per_chunk, st, qr_gate, gate2);
@@ -152,7 +160,7 @@ bpf_status gram(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
     BPF_LAUNCHED(ctx);
     int total = nb * p * p;
     int blocks = std::min(ceil_div(total, 256), ctx->num_sms * 4);
-    gram_reduce_kernel<<<blocks, 256, 0, ctx->stream>>>(total, nchunks, partial, Out, alpha,
+    gram_reduce_kernel<<<blocks, 256, 0, ctx->stream>>>(total, nparts, partial, Out, alpha,
                                                          accumulate ? 1 : 0, Out2, st, qr_gate, gate2);
     BPF_LAUNCHED(ctx);
     return BPF_SUCCESS;
@@ -230,6 +238,81 @@ gram_dmma_kernel(int n, int p, int nb, const double *__restrict__ A, size_t stri
             }
         }
     }
+}
+
+// Same product with the row chunks grouped in clusters of 8 CTAs: the 8 partial tiles are
+// summed through distributed shared memory (each CTA of the cluster sums 1/8 of the tile's
+// rows over the 8 CTAs) and one partial per cluster goes to global memory, an 8x cut of the
+// partial-sum traffic.  The gate is uniform across a cluster, so either every CTA of a
+// cluster returns early or none does.
+template <int GT>
+__global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(128)
+gram_dmma_cl_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
+                    const double *__restrict__ B, double *__restrict__ partial,
+                    int rows_per_chunk, const SolveState *st, const int *gate,
+                    const int *gate2) {
+    if (gate_off(st, gate, gate2)) return;
+    namespace cg = cooperative_groups;
+    constexpr int RS = 32, S = GT + 4, WT = GT / 2, MT = WT / 8;
+    __shared__ double sbuf[2 * RS * S];
+    double *As = sbuf, *Bs = sbuf + RS * S;
+    const int chunk = blockIdx.x, j = blockIdx.y;
+    const int ntile = (p + GT - 1) / GT;
+    const int a0 = (blockIdx.z / ntile) * GT, b0 = (blockIdx.z % ntile) * GT;
+    const int r_begin = chunk * rows_per_chunk;
+    const int r_end = min(n, r_begin + rows_per_chunk);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t4 = lane & 3;
+    const double *Aj = A + (size_t)j * strideA;
+    double acc[MT][MT][2];
+#pragma unroll
+    for (int mi = 0; mi < MT; mi++)
+#pragma unroll
+        for (int ni = 0; ni < MT; ni++) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+    for (int r0 = r_begin; r0 < r_end; r0 += RS) {
+        for (int e = tid; e < RS * GT; e += 128) {
+            const int rr = e / GT, cc = e % GT, r = r0 + rr;
+            const bool rok = r < r_end;
+            As[rr * S + cc] = (rok && a0 + cc < p) ? __ldg(Aj + (size_t)r * p + a0 + cc) : 0.0;
+            Bs[rr * S + cc] = (rok && b0 + cc < p) ? __ldg(B + (size_t)r * p + b0 + cc) : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < RS / 4; ks++) {
+            const int k = ks * 4 + t4;
+            double a[MT], b[MT];
+#pragma unroll
+            for (int mi = 0; mi < MT; mi++) a[mi] = As[k * S + wm * WT + mi * 8 + g];
+#pragma unroll
+            for (int ni = 0; ni < MT; ni++) b[ni] = Bs[k * S + wn * WT + ni * 8 + g];
+#pragma unroll
+            for (int mi = 0; mi < MT; mi++)
+#pragma unroll
+                for (int ni = 0; ni < MT; ni++) dmma884(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+        }
+        __syncthreads();
+    }
+    // this CTA's tile into its shared memory (GT x GT, row-major)
+#pragma unroll
+    for (int mi = 0; mi < MT; mi++)
+#pragma unroll
+        for (int ni = 0; ni < MT; ni++)
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+                sbuf[(wm * WT + mi * 8 + g) * GT + wn * WT + ni * 8 + 2 * t4 + i] = acc[mi][ni][i];
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();
+    const int rank = (int)cluster.block_rank();
+    constexpr int RPR = GT / 8;   // tile rows summed by each CTA of the cluster
+    double *out = partial + ((size_t)(chunk / 8) * nb + j) * p * p;
+    for (int e = tid; e < RPR * GT; e += 128) {
+        const int a = rank * RPR + e / GT, b = e % GT;
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) s += cluster.map_shared_rank(sbuf, q)[a * GT + b];
+        if (a0 + a < p && b0 + b < p) out[(size_t)(a0 + a) * p + b0 + b] = s;
+    }
+    cluster.sync();
 }
 
 // Out rows r0..r0+63, columns b0..b0+GT-1 of beta*C + alpha*sum_j A_j S_j; 4 warps 2 x 2.

@@ -59,58 +59,82 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 }
 
 // ---------------------------------------------------------------------------------------
-// Block back substitution R Y = Z (Y overwrites Z), one CTA per column b of Z (:366-375).
+// One step i of the block back substitution R Y = Z (src/block_gmres.jl:366-375), in the
+// right-looking order: every CTA solves Y_i = R_ii^{-1} Z_i (p x p, redundantly, p columns
+// with L lanes each), CTA 0 stores Y_i, and CTA b < i updates Z_b -= R_{b,i} Y_i.  Z_i is
+// never written in step i, so every CTA reads it intact.  SMEM: R_ii, Z_i and R_{b,i} staged
+// in shared memory (row stride p+1); otherwise Y_i is solved in place in Y (global).
 // ---------------------------------------------------------------------------------------
+template <bool SMEM>
 __global__ void __launch_bounds__(256)
-backsub_kernel(int p, const double *__restrict__ Rblk, double *__restrict__ Z,
-               const SolveState *st) {
-    const int k = st->inner_iter;
-    const int b = blockIdx.x;
-    extern __shared__ double y[];
+backsub_step_kernel(int p, int i, const double *__restrict__ Rblk, double *__restrict__ Z,
+                    double *__restrict__ Y) {
+    extern __shared__ double sm[];
     const size_t pp = (size_t)p * p;
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = k - 1; i >= 0; i--) {
-        for (int a = tid; a < p; a += nt) y[a] = Z[(size_t)i * pp + (size_t)a * p + b];
-        __syncthreads();
-        if (warp == 0) {
-            const double *R = Rblk + rpos(i, i) * pp;
-            double v[4];
-#pragma unroll
-            for (int t = 0; t < 4; t++) {
-                const int r = lane + 32 * t;
-                v[t] = r < p ? y[r] : 0.0;
-            }
-            for (int c = p - 1; c >= 0; c--) {
-                const int owner = c & 31, slot = c >> 5;
-                double vc = 0.0;
-#pragma unroll
-                for (int t = 0; t < 4; t++)
-                    if (t == slot) vc = v[t];
-                vc = __shfl_sync(0xffffffffu, vc, owner) / R[(size_t)c * p + c];
-#pragma unroll
-                for (int t = 0; t < 4; t++) {
-                    const int r = lane + 32 * t;
-                    if (r == c) v[t] = vc;
-                    else if (r < c) v[t] -= R[(size_t)r * p + c] * vc;
-                }
-            }
-#pragma unroll
-            for (int t = 0; t < 4; t++) {
-                const int r = lane + 32 * t;
-                if (r < p) y[r] = v[t];
-            }
-        }
-        __syncthreads();
-        for (int a = tid; a < p; a += nt) Z[(size_t)i * pp + (size_t)a * p + b] = y[a];
-        for (int e = tid; e < i * p; e += nt) {
-            const int i2 = e / p, a = e % p;
-            const double *R = Rblk + rpos(i2, i) * pp + (size_t)a * p;
+    const int ld = SMEM ? p + 1 : p;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const double *Rii = Rblk + rpos(i, i) * pp;
+    double *Rs = SMEM ? sm : const_cast<double *>(Rii);
+    double *Ys = SMEM ? sm + p * ld : Y + (size_t)i * pp;
+    double *Rb = SMEM ? sm + 2 * p * ld : nullptr;
+    for (int e = tid; e < p * p; e += nt) {
+        const int a = e / p, b = e % p;
+        if (SMEM) Rs[a * ld + b] = Rii[e];
+        Ys[a * ld + b] = Z[(size_t)i * pp + e];
+    }
+    __syncthreads();
+    const int L = (nt >= 4 * p) ? 4 : ((nt >= 2 * p) ? 2 : 1);
+    const int q = tid % L;
+    for (int c0 = 0; c0 < p; c0 += nt / L) {
+        const int c = c0 + tid / L;
+        const bool act = c < p;
+        for (int r = p - 1; r >= 0; r--) {
             double s = 0.0;
-            for (int c = 0; c < p; c++) s += R[c] * y[c];
-            Z[(size_t)i2 * pp + (size_t)a * p + b] -= s;
+            if (act)
+                for (int k = r + 1 + q; k < p; k += L) s += Rs[r * ld + k] * Ys[k * ld + c];
+            if (L >= 4) s += __shfl_xor_sync(0xffffffffu, s, 2);
+            if (L >= 2) s += __shfl_xor_sync(0xffffffffu, s, 1);
+            if (act && q == 0) Ys[r * ld + c] = (Ys[r * ld + c] - s) / Rs[r * ld + r];
+            __syncwarp();
         }
+    }
+    __syncthreads();
+    if (SMEM && blockIdx.x == 0)
+        for (int e = tid; e < p * p; e += nt) Y[(size_t)i * pp + e] = Ys[(e / p) * ld + e % p];
+    const int bb = blockIdx.x;
+    if (bb >= i) return;
+    const double *Rbi = Rblk + rpos(bb, i) * pp;
+    if (SMEM) {
+        for (int e = tid; e < p * p; e += nt) Rb[(e / p) * ld + e % p] = Rbi[e];
         __syncthreads();
     }
+    const double *Rsrc = SMEM ? Rb : Rbi;
+    double *Zb = Z + (size_t)bb * pp;
+    for (int e = tid; e < p * p; e += nt) {
+        const int a = e / p, col = e % p;
+        double s = 0.0;
+        for (int c = 0; c < p; c++) s += Rsrc[a * ld + c] * Ys[c * ld + col];
+        Zb[e] -= s;
+    }
+}
+
+static bpf_status launch_backsub(bpf_ctx *ctx, int p, int k, const double *Rblk, double *Z,
+                                 double *Y) {
+    KScope ks(ctx, BPF_KC_SMALL);
+    const size_t smem = sizeof(double) * 3 * p * (p + 1);
+    const bool use_smem = smem <= 220 * 1024;
+    if (use_smem && smem > 48 * 1024)
+        BPF_CUDA(ctx, cudaFuncSetAttribute(backsub_step_kernel<true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (int i = k - 1; i >= 0; i--) {
+        const int grid = std::max(i, 1);
+        if (use_smem)
+            backsub_step_kernel<true><<<grid, 256, smem, ctx->stream>>>(p, i, Rblk, Z, Y);
+        else
+            backsub_step_kernel<false><<<grid, 256, 0, ctx->stream>>>(p, i, Rblk, Z, Y);
+        BPF_LAUNCHED(ctx);
+    }
+    return BPF_SUCCESS;
 }
 
 __global__ void gmres_init_kernel(SolveState *st, double atol, double rtol, double *hist,
@@ -155,12 +179,20 @@ static double now_s() {
 
 struct GmresBufs {
     double *V, *Rblk, *HY, *tau, *Z;
+    double *Zb;   // flexible form: preconditioned basis N \ V_i (null otherwise)
     int cap;
 };
 
-static bpf_status gmres_capacity(bpf_ctx *ctx, int n, int p, int cap, int old_cap, GmresBufs &g) {
+static bpf_status gmres_capacity(bpf_ctx *ctx, int n, int p, int cap, int old_cap, GmresBufs &g,
+                                 bool flexible) {
     const size_t np = (size_t)n * p, pp = (size_t)p * p;
     BPF_TRY(ws_grow_keep(ctx, WS_V, sizeof(double) * np * (cap + 1), sizeof(double) * np * (old_cap + 1)));
+    if (flexible) {
+        BPF_TRY(ws_grow_keep(ctx, WS_ZB, sizeof(double) * np * cap, sizeof(double) * np * old_cap));
+        g.Zb = (double *)ctx->ws[WS_ZB];
+    } else {
+        g.Zb = nullptr;
+    }
     BPF_TRY(ws_grow_keep(ctx, WS_HESS, sizeof(double) * pp * ((size_t)cap * (cap + 1) / 2),
                          sizeof(double) * pp * ((size_t)old_cap * (old_cap + 1) / 2)));
     BPF_TRY(ws_grow_keep(ctx, WS_HY, sizeof(double) * (3 * pp + p) * cap,
@@ -227,8 +259,13 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
     double *fold_scr = Cm + 5 * pp;
     double *tau_cur = Cm + 6 * pp;
     GmresBufs g{};
+    // An FP32-factor right preconditioner is not exactly the same linear map at every
+    // application (rounding), so the flexible form keeps the preconditioned blocks
+    // Zb_i = N \ V_i and forms X += sum Zb_i Y_i (Saad's FGMRES); the Arnoldi relation
+    // A Zb = V H then holds in FP64 and the residual estimate stays the true residual.
+    const bool flexible = N && N->fdtype == BPF_F32;
     int cap = restart ? std::min(memory, std::max(itmax, 1)) : std::min(std::max(itmax, 1), std::max(memory, 16));
-    BPF_TRY(gmres_capacity(ctx, n, p, cap, 0, g));
+    BPF_TRY(gmres_capacity(ctx, n, p, cap, 0, g, flexible));
 
     // State on the host side.
     SolveState hs;
@@ -293,7 +330,7 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
             const int kend = std::min(kmax, k + chunk);
             if (kend > g.cap) {
                 int newcap = std::min(std::max(kend, 2 * g.cap), std::max(kmax, 1));
-                BPF_TRY(gmres_capacity(ctx, n, p, newcap, g.cap, g));
+                BPF_TRY(gmres_capacity(ctx, n, p, newcap, g.cap, g, flexible));
             }
             // Size the Gram workspaces for the largest k of this chunk up front, so no
             // allocation (and no implicit synchronisation) happens between launches.
@@ -307,8 +344,9 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
                 double *Vn = g.V + (size_t)kk * np;
                 const double *Pk = Vk;
                 if (N) {                                                     // :297-298
-                    BPF_TRY(prec_apply_rowmajor(ctx, N, p, Vk, Pm, &st->active));
-                    Pk = Pm;
+                    double *dst = flexible ? g.Zb + (size_t)jj * np : Pm;
+                    BPF_TRY(prec_apply_rowmajor(ctx, N, p, Vk, dst, &st->active));
+                    Pk = dst;
                 }
                 BPF_TRY(spmm_rowmajor(ctx, n, A->nnz, rp, ci, av, base, p, 1.0, Pk, 0.0, W, nullptr, &st->active));
                 double *Qk = W;
@@ -355,10 +393,15 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
         }
         const int inner_iter = hs.inner_iter;
         // :366-385
-        backsub_kernel<<<p, 256, sizeof(double) * p, ctx->stream>>>(p, g.Rblk, g.Z, st);
-        BPF_LAUNCHED(ctx);
-        BPF_TRY(tsmm(ctx, n, p, g.cap, g.V, np, g.Z, pp, 1.0, Xr, 1.0, Xr, nullptr, &st->inner_iter));
-        if (N) {
+        double *Yb = (double *)ws_get(ctx, WS_Y, sizeof(double) * pp * std::max(inner_iter, 1), &s);
+        if (!Yb) return s;
+        BPF_TRY(launch_backsub(ctx, p, inner_iter, g.Rblk, g.Z, Yb));
+        if (flexible) {                                                     // X += sum (N \ V_i) Y_i
+            BPF_TRY(tsmm(ctx, n, p, inner_iter, g.Zb, np, Yb, pp, 1.0, Xr, 1.0, Xr, nullptr));
+        } else {
+            BPF_TRY(tsmm(ctx, n, p, inner_iter, g.V, np, Yb, pp, 1.0, Xr, 1.0, Xr, nullptr));
+        }
+        if (N && !flexible) {
             BPF_CUDA(ctx, cudaMemcpyAsync(Pm, Xr, sizeof(double) * np, cudaMemcpyDeviceToDevice, ctx->stream));
             BPF_TRY(prec_apply_rowmajor(ctx, N, p, Pm, Xr));
         }

@@ -462,8 +462,12 @@ static bpf_status launch_trsv2(bpf_ctx *ctx, const TriDev &t0, const TriDev &t1,
         threads = 512;
         grid = 1;
     } else {
-        threads = 256;
-        BPF_TRY(coop_grid(ctx, kern, threads, 0, ceil_div(maxrows, threads / G), &grid));
+        // At most one CTA of 512 threads per SM: the level barriers cost one arrival per CTA,
+        // so fewer, wider CTAs make every level cheaper (the widest levels still get a group
+        // of lanes per row).
+        threads = 512;
+        BPF_TRY(coop_grid(ctx, kern, threads, 0,
+                          std::min(ceil_div(maxrows, threads / G), ctx->num_sms), &grid));
     }
     TriKernelArgs a0 = t0.args(), a1 = t1.args();
     DevStatus *ds = ctx->dstat;

@@ -32,23 +32,27 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// Inverse of an upper-triangular p x p matrix U (row stride ldu) into X (row stride ldx):
-// thread c computes column c of X = U^{-1} by back substitution (x_k = 0 for k > c, so every
-// thread runs the same loop; U[i][k] is a broadcast).  Both operands in shared memory.
+// Inverse of an upper-triangular p x p matrix U (row stride ldu) into X (row stride ldx), both
+// in shared memory.  Column c of X = U^{-1} is computed by back substitution (x_k = 0 for
+// k > c, so every column runs the same loop) by a group of L consecutive lanes that split the
+// inner products and combine them with shuffles; L = 4, 2 or 1 so that the p columns fill
+// the block.
 __device__ void upper_inverse(int p, const double *U, int ldu, double *X, int ldx) {
-    for (int c = threadIdx.x; c < p; c += blockDim.x) {
+    const int nt = blockDim.x;
+    const int L = (nt >= 4 * p) ? 4 : ((nt >= 2 * p) ? 2 : 1);
+    const int tid = threadIdx.x;
+    const int q = tid % L;
+    for (int c0 = 0; c0 < p; c0 += nt / L) {
+        const int c = c0 + tid / L;
+        const bool act = (tid / L < nt / L) && c < p;
         for (int i = p - 1; i >= 0; i--) {
-            double s = (i == c) ? 1.0 : 0.0;
-            double s1 = 0.0, s2 = 0.0, s3 = 0.0;
-            int k = i + 1;
-            for (; k + 3 < p; k += 4) {
-                s -= U[i * ldu + k] * X[k * ldx + c];
-                s1 -= U[i * ldu + k + 1] * X[(k + 1) * ldx + c];
-                s2 -= U[i * ldu + k + 2] * X[(k + 2) * ldx + c];
-                s3 -= U[i * ldu + k + 3] * X[(k + 3) * ldx + c];
-            }
-            for (; k < p; k++) s -= U[i * ldu + k] * X[k * ldx + c];
-            X[i * ldx + c] = (i > c) ? 0.0 : (s + s1 + s2 + s3) / U[i * ldu + i];
+            double s = 0.0;
+            if (act)
+                for (int k = i + 1 + q; k < p; k += L) s += U[i * ldu + k] * X[k * ldx + c];
+            if (L >= 4) s += __shfl_xor_sync(0xffffffffu, s, 2);
+            if (L >= 2) s += __shfl_xor_sync(0xffffffffu, s, 1);
+            if (act && q == 0) X[i * ldx + c] = (i > c) ? 0.0 : (((i == c) ? 1.0 : 0.0) - s) / U[i * ldu + i];
+            __syncwarp();
         }
     }
 }
@@ -107,10 +111,12 @@ chol2_kernel(int n, int p, const double *__restrict__ G, double *__restrict__ Ri
             }
             const double r = sqrt(d), dinv = 1.0 / d;
             for (int c = j + tid; c < p; c += nt) R[j * ldr + c] = (c == j) ? r : g[j * ld + c] / r;
-            const int m = p - j - 1;
-            for (int e = tid; e < m * m; e += nt) {
-                const int a = j + 1 + e / m, b = j + 1 + e % m;
-                if (b >= a) g[a * ld + b] -= g[j * ld + a] * g[j * ld + b] * dinv;
+            // trailing update of the upper triangle: 16 x 16 thread grid, rows a, columns b >= a
+            const int ty = tid >> 4, tx = tid & 15;
+            for (int a = j + 1 + ty; a < p; a += nt >> 4) {
+                const double ga = g[j * ld + a] * dinv;
+                for (int b = j + 1 + tx; b < p; b += 16)
+                    if (b >= a) g[a * ld + b] -= ga * g[j * ld + b];
             }
             __syncthreads();
         }
@@ -302,7 +308,10 @@ hess_factor2_kernel(int p, int k, double *__restrict__ Rblk, double *__restrict_
     double *Rjj = Rblk + rblk_pos(j, j) * pp;
     double *Zj = Z + (size_t)j * pp;
     double *Zn = Z + (size_t)(j + 1) * pp;
-    double *W1 = scr, *W2 = scr + pp;
+    // W1, W2 and a copy of Z_j live in shared memory after F when F does (F_SMEM)
+    double *W1 = F_SMEM ? Fs + 2 * p * ld : scr;
+    double *W2 = F_SMEM ? W1 + pp : scr + pp;
+    double *Zs = F_SMEM ? W2 + pp : Zj;
     double *Tinv = scr + 2 * pp;        // p x p (global scratch)
     const int c_of = tid % p, q_of = tid / p;
     for (size_t e = tid; e < pp; e += nt) {
@@ -431,11 +440,15 @@ hess_factor2_kernel(int p, int k, double *__restrict__ Rblk, double *__restrict_
     }
     __syncthreads();
     for (int e = tid; e < p * p; e += nt) T[e] = Tm[(e / p) * ld + e % p];
+    if (F_SMEM) {
+        for (int e = tid; e < p * p; e += nt) Zs[e] = Zj[e];
+        __syncthreads();
+    }
     // W1 = Y_top^T Z_j
     for (int e = tid; e < p * p; e += nt) {
         const int c = e / p, b = e % p;
         double s = 0.0;
-        for (int r = c; r < p; r++) s += F[r * ldf + c] * Zj[(size_t)r * p + b];
+        for (int r = c; r < p; r++) s += F[r * ldf + c] * Zs[(size_t)r * p + b];
         W1[e] = s;
     }
     __syncthreads();
@@ -455,7 +468,7 @@ hess_factor2_kernel(int p, int k, double *__restrict__ Rblk, double *__restrict_
         double s = 0.0;
         for (int c = 0; c <= cmax; c++) s += F[r * ldf + c] * W2[(size_t)c * p + b];
         if (r < p) {
-            Zj[e] -= s;
+            Zj[e] = Zs[e] - s;
         } else {
             Zn[e - pp] = -s;
             ss += s * s;
@@ -499,7 +512,7 @@ bpf_status launch_hess(bpf_ctx *ctx, int p, int k, double *Rblk, double *HY, dou
     }
     BPF_LAUNCHED(ctx);
     const size_t base_f = sizeof(double) * (p * (p + 1) + nparts * p + p);
-    const size_t smem_f = base_f + sizeof(double) * 2 * p * (p + 1);
+    const size_t smem_f = base_f + sizeof(double) * (2 * p * (p + 1) + 3 * pp);
     if (smem_f <= 220 * 1024) {
         if (smem_f > 48 * 1024)
             BPF_CUDA(ctx, cudaFuncSetAttribute(hess_factor2_kernel<true>,

@@ -144,5 +144,29 @@ def test_gmres_benchmark_dump_case300(dump300, bpf):
     X, st = bpf.block_gmres(Ad, _t(Gu), N=bpf.ilu0(Ad, 64), ldiv=True, memory=8, restart=True,
                             atol=0.0, rtol=1e-13, itmax=400)
     assert st.solved
+    # Gx of case300 has kappa ~1e4: a 1e-13 residual bounds the forward error by ~1e-9, so the
+    # comparison with the direct solve uses that bound (the 1e-10 agreement is shown on J with
+    # rtol 1e-13 in test_gmres_matches_direct_tight).
     Xd = z["X"][:, :64]
-    assert np.linalg.norm(X.cpu().numpy() - Xd) <= 1e-10 * np.linalg.norm(Xd)
+    assert np.linalg.norm(X.cpu().numpy() - Xd) <= 1e-9 * np.linalg.norm(Xd)
+
+
+@pytest.mark.parametrize("n_bus,p", [(300, 16), (1000, 64)])
+def test_gmres_fp32_factors_flexible_reaches_fp64_residual(bpf, n_bus, p):
+    """Mixed precision: FP32 ILU0 factors and triangular solves inside FP64 flexible GMRES.
+    The true FP64 residual reaches the same 1e-8 as the plain FP64 solve, in about as many
+    iterations (ILU0's own error dwarfs FP32 rounding)."""
+    A = bpf.grid.synthetic_jacobian(n_bus, 68 if n_bus == 300 else 110, 0)
+    B = bpf.grid.gaussian_rhs(A.shape[0], p, 1)
+    Ad = _dev(A, bpf)
+    X64, s64 = bpf.block_gmres(Ad, _t(B), N=bpf.ilu0(Ad, p), ldiv=True, restart=False,
+                               memory=200, atol=0.0, rtol=1e-8, itmax=200)
+    X32, s32 = bpf.block_gmres(Ad, _t(B), N=bpf.ilu0(Ad, p, factor_dtype="float32"), ldiv=True,
+                               restart=False, memory=200, atol=0.0, rtol=1e-8, itmax=200)
+    assert s64.solved and s32.solved
+    assert s32.niter <= s64.niter + 2
+    rel = np.linalg.norm(B - A @ X32.cpu().numpy()) / np.linalg.norm(B)
+    assert rel <= 1.05e-8
+    Xd = np.linalg.solve(A.toarray(), B) if A.shape[0] <= 2000 else None
+    if Xd is not None:
+        assert np.linalg.norm(X32.cpu().numpy() - Xd) / np.linalg.norm(Xd) <= 1e-4
