@@ -321,7 +321,7 @@ def main():
         launches = bpf.kernel_launches() - l0
         t_ms = sum(a.elapsed_time(b) for a, b in ev)
         kern = {}
-        for kc in ("spmm", "trsv", "factor", "gram", "tsmm", "small"):
+        for kc in ("spmm", "trsv", "factor", "gram", "tsmm", "small", "chol", "hess", "backsub"):
             ms, cnt, by, fl = bpf._lib.kernel_time(kc)
             kern[kc] = {"ms": ms, "launches": cnt, "bytes": by, "flops": fl}
         bpf._lib.set_timing(False)

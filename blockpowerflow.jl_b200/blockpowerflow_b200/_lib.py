@@ -176,7 +176,8 @@ def kernel_launches(device=None) -> int:
     return int(load().bpf_ctx_kernel_launches(context(device)))
 
 
-KERNEL_CLASSES = {"spmm": 0, "trsv": 1, "factor": 2, "gram": 3, "tsmm": 4, "small": 5}
+KERNEL_CLASSES = {"spmm": 0, "trsv": 1, "factor": 2, "gram": 3, "tsmm": 4, "small": 5,
+                  "chol": 6, "hess": 7, "backsub": 8}
 
 
 def set_timing(on: bool, device=None) -> None:

@@ -500,9 +500,9 @@ bpf_status cholqr(bpf_ctx *ctx, int n, int p, const double *W, double *Q, double
                   double *T, SolveState *st, const int *gate, int *shift_flag, int *reorth_flag) {
     if (p > 128) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "Cholesky-QR: p=%d > 128", p);
     bpf_status s;
-    double *small = (double *)ws_get(ctx, WS_SMALL, sizeof(double) * 3 * p * p, &s);
+    double *small = (double *)ws_get(ctx, WS_SMALL, sizeof(double) * 4 * p * p, &s);
     if (!small) return s;
-    double *G = small, *Rinv = small + p * p, *Rtmp = small + 2 * p * p;
+    double *G = small, *Rinv = small + p * p, *Rtmp = small + 2 * p * p;   // Rtmp: 2 p x p
     if (!shift_flag) shift_flag = &st->qr_shift;
     const int *g3 = shift_flag;
     // pass 1: W -> T

@@ -33,7 +33,6 @@
 
 namespace bpf {
 
-__host__ __device__ inline size_t rpos(int i, int j) { return (size_t)j * (j + 1) / 2 + i; }
 
 __device__ __forceinline__ double block_sum(double v, double *red) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -56,85 +55,6 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
-}
-
-// ---------------------------------------------------------------------------------------
-// One step i of the block back substitution R Y = Z (src/block_gmres.jl:366-375), in the
-// right-looking order: every CTA solves Y_i = R_ii^{-1} Z_i (p x p, redundantly, p columns
-// with L lanes each), CTA 0 stores Y_i, and CTA b < i updates Z_b -= R_{b,i} Y_i.  Z_i is
-// never written in step i, so every CTA reads it intact.  SMEM: R_ii, Z_i and R_{b,i} staged
-// in shared memory (row stride p+1); otherwise Y_i is solved in place in Y (global).
-// ---------------------------------------------------------------------------------------
-template <bool SMEM>
-__global__ void __launch_bounds__(256)
-backsub_step_kernel(int p, int i, const double *__restrict__ Rblk, double *__restrict__ Z,
-                    double *__restrict__ Y) {
-    extern __shared__ double sm[];
-    const size_t pp = (size_t)p * p;
-    const int ld = SMEM ? p + 1 : p;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const double *Rii = Rblk + rpos(i, i) * pp;
-    double *Rs = SMEM ? sm : const_cast<double *>(Rii);
-    double *Ys = SMEM ? sm + p * ld : Y + (size_t)i * pp;
-    double *Rb = SMEM ? sm + 2 * p * ld : nullptr;
-    for (int e = tid; e < p * p; e += nt) {
-        const int a = e / p, b = e % p;
-        if (SMEM) Rs[a * ld + b] = Rii[e];
-        Ys[a * ld + b] = Z[(size_t)i * pp + e];
-    }
-    __syncthreads();
-    const int L = (nt >= 4 * p) ? 4 : ((nt >= 2 * p) ? 2 : 1);
-    const int q = tid % L;
-    for (int c0 = 0; c0 < p; c0 += nt / L) {
-        const int c = c0 + tid / L;
-        const bool act = c < p;
-        for (int r = p - 1; r >= 0; r--) {
-            double s = 0.0;
-            if (act)
-                for (int k = r + 1 + q; k < p; k += L) s += Rs[r * ld + k] * Ys[k * ld + c];
-            if (L >= 4) s += __shfl_xor_sync(0xffffffffu, s, 2);
-            if (L >= 2) s += __shfl_xor_sync(0xffffffffu, s, 1);
-            if (act && q == 0) Ys[r * ld + c] = (Ys[r * ld + c] - s) / Rs[r * ld + r];
-            __syncwarp();
-        }
-    }
-    __syncthreads();
-    if (SMEM && blockIdx.x == 0)
-        for (int e = tid; e < p * p; e += nt) Y[(size_t)i * pp + e] = Ys[(e / p) * ld + e % p];
-    const int bb = blockIdx.x;
-    if (bb >= i) return;
-    const double *Rbi = Rblk + rpos(bb, i) * pp;
-    if (SMEM) {
-        for (int e = tid; e < p * p; e += nt) Rb[(e / p) * ld + e % p] = Rbi[e];
-        __syncthreads();
-    }
-    const double *Rsrc = SMEM ? Rb : Rbi;
-    double *Zb = Z + (size_t)bb * pp;
-    for (int e = tid; e < p * p; e += nt) {
-        const int a = e / p, col = e % p;
-        double s = 0.0;
-        for (int c = 0; c < p; c++) s += Rsrc[a * ld + c] * Ys[c * ld + col];
-        Zb[e] -= s;
-    }
-}
-
-static bpf_status launch_backsub(bpf_ctx *ctx, int p, int k, const double *Rblk, double *Z,
-                                 double *Y) {
-    KScope ks(ctx, BPF_KC_SMALL);
-    const size_t smem = sizeof(double) * 3 * p * (p + 1);
-    const bool use_smem = smem <= 220 * 1024;
-    if (use_smem && smem > 48 * 1024)
-        BPF_CUDA(ctx, cudaFuncSetAttribute(backsub_step_kernel<true>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    for (int i = k - 1; i >= 0; i--) {
-        const int grid = std::max(i, 1);
-        if (use_smem)
-            backsub_step_kernel<true><<<grid, 256, smem, ctx->stream>>>(p, i, Rblk, Z, Y);
-        else
-            backsub_step_kernel<false><<<grid, 256, 0, ctx->stream>>>(p, i, Rblk, Z, Y);
-        BPF_LAUNCHED(ctx);
-    }
-    return BPF_SUCCESS;
 }
 
 __global__ void gmres_init_kernel(SolveState *st, double atol, double rtol, double *hist,
@@ -195,8 +115,8 @@ static bpf_status gmres_capacity(bpf_ctx *ctx, int n, int p, int cap, int old_ca
     }
     BPF_TRY(ws_grow_keep(ctx, WS_HESS, sizeof(double) * pp * ((size_t)cap * (cap + 1) / 2),
                          sizeof(double) * pp * ((size_t)old_cap * (old_cap + 1) / 2)));
-    BPF_TRY(ws_grow_keep(ctx, WS_HY, sizeof(double) * (3 * pp + p) * cap,
-                         sizeof(double) * (3 * pp + p) * old_cap));
+    BPF_TRY(ws_grow_keep(ctx, WS_HY, sizeof(double) * hy_stride(p) * cap,
+                         sizeof(double) * hy_stride(p) * old_cap));
     BPF_TRY(ws_grow_keep(ctx, WS_Z, sizeof(double) * pp * (cap + 1), sizeof(double) * pp * (old_cap + 1)));
     g.V = (double *)ctx->ws[WS_V];
     g.Rblk = (double *)ctx->ws[WS_HESS];
@@ -354,7 +274,7 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
                     BPF_TRY(prec_apply_rowmajor(ctx, M, p, W, Qm, &st->active));
                     Qk = Qm;
                 }
-                double *Psi = g.Rblk + rpos(0, jj) * pp;                     // :301-313
+                double *Psi = g.Rblk + rblk_pos(0, jj) * pp;                     // :301-313
                 BPF_TRY(gram(ctx, n, p, kk, g.V, np, Qk, Psi, 1.0, false, st));
                 BPF_TRY(tsmm(ctx, n, p, kk, g.V, np, Psi, pp, -1.0, Qk, 1.0, Qk, st));
                 BPF_TRY(gram(ctx, n, p, kk, g.V, np, Qk, Psi, 1.0, true, st, nullptr, Psi2buf));
@@ -395,7 +315,7 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
         // :366-385
         double *Yb = (double *)ws_get(ctx, WS_Y, sizeof(double) * pp * std::max(inner_iter, 1), &s);
         if (!Yb) return s;
-        BPF_TRY(launch_backsub(ctx, p, inner_iter, g.Rblk, g.Z, Yb));
+        BPF_TRY(launch_backsub(ctx, p, inner_iter, g.Rblk, g.HY, g.Z, Yb));
         if (flexible) {                                                     // X += sum (N \ V_i) Y_i
             BPF_TRY(tsmm(ctx, n, p, inner_iter, g.Zb, np, Yb, pp, 1.0, Xr, 1.0, Xr, nullptr));
         } else {

@@ -137,8 +137,11 @@ typedef enum {
     BPF_KC_FACTOR = 2,  /* ILU0 / IC0 / RF numeric factorization      */
     BPF_KC_GRAM = 3,    /* block Gram products (split over rows)      */
     BPF_KC_TSMM = 4,    /* tall x small block products                */
-    BPF_KC_SMALL = 5,   /* one-CTA p x p kernels (Cholesky, Hessenberg) */
-    BPF_KC_COUNT = 6
+    BPF_KC_SMALL = 5,   /* other one-CTA p x p kernels (BiCGSTAB solves) */
+    BPF_KC_CHOL = 6,    /* Cholesky-QR: Cholesky + inverse of p x p Gram */
+    BPF_KC_HESS = 7,    /* block Hessenberg QR update (apply + factor) */
+    BPF_KC_BACKSUB = 8, /* block back substitution of block-GMRES     */
+    BPF_KC_COUNT = 9
 } bpf_kernel_class;
 BPF_API bpf_status bpf_ctx_set_timing(bpf_ctx *ctx, int on);
 /* Totals since bpf_ctx_set_timing(ctx, 1): device milliseconds, launches, and the launches'
