@@ -201,9 +201,24 @@ bpf_status bpf_ctx_create(bpf_ctx **out, void *stream) {
     if (e == cudaSuccess) e = cudaMalloc((void **)&ctx->dstat, sizeof(DevStatus));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->hstat, sizeof(DevStatus));
     if (e == cudaSuccess) e = cudaMemset(ctx->dstat, 0, sizeof(DevStatus));
+    if (const char *env = getenv("BPF_OVERLAP")) ctx->overlap = atoi(env) != 0;
+    if (e == cudaSuccess) {
+        int least = 0, greatest = 0;
+        e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&ctx->hstream, cudaStreamNonBlocking, greatest);
+    }
+    for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+        e = cudaEventCreateWithFlags(&ctx->ev_a[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_b[i], cudaEventDisableTiming);
+    }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         cudaGetLastError();
+        for (int i = 0; i < 2; i++) {
+            if (ctx->ev_a[i]) cudaEventDestroy(ctx->ev_a[i]);
+            if (ctx->ev_b[i]) cudaEventDestroy(ctx->ev_b[i]);
+        }
+        if (ctx->hstream) cudaStreamDestroy(ctx->hstream);
         if (ctx->dstat) cudaFree(ctx->dstat);
         if (ctx->hstat) cudaFreeHost(ctx->hstat);
         delete ctx;
@@ -222,7 +237,13 @@ bpf_status bpf_ctx_set_stream(bpf_ctx *ctx, void *stream) {
 bpf_status bpf_ctx_destroy(bpf_ctx *ctx) {
     if (!ctx) return BPF_SUCCESS;
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->hstream) cudaStreamSynchronize(ctx->hstream);
     for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+    for (int i = 0; i < 2; i++) {
+        if (ctx->ev_a[i]) cudaEventDestroy(ctx->ev_a[i]);
+        if (ctx->ev_b[i]) cudaEventDestroy(ctx->ev_b[i]);
+    }
+    if (ctx->hstream) cudaStreamDestroy(ctx->hstream);
     for (int s = 0; s < WS_COUNT; s++)
         if (ctx->ws[s]) cudaFree(ctx->ws[s]);
     cudaFree(ctx->dstat);

@@ -71,6 +71,14 @@ struct bpf_ctx {
     // FP64 block products on the tensor pipe (DMMA) instead of FMA; BPF_FP64_MMA=0 turns it
     // off (used to compare the two paths).
     bool fp64_mma = true;
+    // Second (high-priority) stream on which block-GMRES runs the Hessenberg QR update of
+    // iteration k while the main stream runs the Arnoldi step of iteration k+1; events hand
+    // the C blocks over (ev_a) and back (ev_b), double buffered by iteration parity.
+    // BPF_OVERLAP=0 keeps everything on the main stream.
+    bool overlap = true;
+    cudaStream_t hstream = nullptr;
+    cudaEvent_t ev_a[2] = {nullptr, nullptr};
+    cudaEvent_t ev_b[2] = {nullptr, nullptr};
     // per-kernel-class event timing (bpf_ctx_set_timing)
     bool timing = false;
     std::vector<cudaEvent_t> event_pool;
@@ -138,6 +146,14 @@ struct KScope {
             }
         }
     }
+};
+
+// Launches made while it lives go to stream `s` (restored on scope exit, error paths included).
+struct StreamSwap {
+    bpf_ctx *ctx;
+    cudaStream_t saved;
+    StreamSwap(bpf_ctx *c, cudaStream_t s) : ctx(c), saved(c->stream) { ctx->stream = s; }
+    ~StreamSwap() { ctx->stream = saved; }
 };
 
 // ------------------------------------------------------------------------------------

@@ -497,7 +497,8 @@ __global__ void gated_copy_kernel(size_t len, const double *__restrict__ src,
 }
 
 bpf_status cholqr(bpf_ctx *ctx, int n, int p, const double *W, double *Q, double *R,
-                  double *T, SolveState *st, const int *gate, int *shift_flag, int *reorth_flag) {
+                  double *T, SolveState *st, const int *gate, int *shift_flag, int *reorth_flag,
+                  int iter_tag) {
     if (p > 128) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "Cholesky-QR: p=%d > 128", p);
     bpf_status s;
     double *small = (double *)ws_get(ctx, WS_SMALL, sizeof(double) * 4 * p * p, &s);
@@ -507,15 +508,15 @@ bpf_status cholqr(bpf_ctx *ctx, int n, int p, const double *W, double *Q, double
     const int *g3 = shift_flag;
     // pass 1: W -> T
     BPF_TRY(gram(ctx, n, p, 1, W, 0, W, G, 1.0, false, st, gate));
-    BPF_TRY(launch_chol(ctx, n, p, G, Rinv, R, Rtmp, 0, st, gate, nullptr, shift_flag, reorth_flag));
+    BPF_TRY(launch_chol(ctx, n, p, G, Rinv, R, Rtmp, 0, st, gate, nullptr, shift_flag, reorth_flag, iter_tag));
     BPF_TRY(tsmm(ctx, n, p, 1, W, 0, Rinv, 0, 1.0, nullptr, 0.0, T, st, nullptr, gate));
     // pass 2: T -> Q
     BPF_TRY(gram(ctx, n, p, 1, T, 0, T, G, 1.0, false, st, gate));
-    BPF_TRY(launch_chol(ctx, n, p, G, Rinv, R, Rtmp, 1, st, gate, nullptr, shift_flag, nullptr));
+    BPF_TRY(launch_chol(ctx, n, p, G, Rinv, R, Rtmp, 1, st, gate, nullptr, shift_flag, nullptr, iter_tag));
     BPF_TRY(tsmm(ctx, n, p, 1, T, 0, Rinv, 0, 1.0, nullptr, 0.0, Q, st, nullptr, gate));
     // pass 3 (only when a pass needed the shift): Q -> T -> Q
     BPF_TRY(gram(ctx, n, p, 1, Q, 0, Q, G, 1.0, false, st, gate, nullptr, g3));
-    BPF_TRY(launch_chol(ctx, n, p, G, Rinv, R, Rtmp, 2, st, gate, g3, nullptr, nullptr));
+    BPF_TRY(launch_chol(ctx, n, p, G, Rinv, R, Rtmp, 2, st, gate, g3, nullptr, nullptr, iter_tag));
     BPF_TRY(tsmm(ctx, n, p, 1, Q, 0, Rinv, 0, 1.0, nullptr, 0.0, T, st, nullptr, gate, g3));
     size_t len = (size_t)n * p;
     int blocks = std::max(1, std::min(ceil_div((long long)len, 256), ctx->num_sms * 8));

@@ -23,6 +23,8 @@ struct SolveState {
     int qr_fail;
     int qr_reorth;     // the new basis block was ill-conditioned: re-orthogonalize it
     int qr_shift2;     // shift flag of the re-orthogonalization's Cholesky-QR
+    int qr_fail_iter;  // smallest tagged iteration whose Cholesky-QR broke down (INT_MAX: none)
+    int pad1;
     double eps;
     double rnorm;
     double atol, rtol;
@@ -55,9 +57,11 @@ bpf_status tsmm(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
 //   shift_flag: set by the first pass when it needed the shift (default st->qr_shift).
 //   reorth_flag (nullable): set when the first Cholesky lost more than 8 digits on some
 //   column (the block was ill-conditioned; its Q should be re-orthogonalized).
+//   iter_tag >= 0: a breakdown records min(st->qr_fail_iter, iter_tag) instead of raising the
+//   context's device error (block-GMRES decides on the host whether that iteration counted).
 bpf_status cholqr(bpf_ctx *ctx, int n, int p, const double *W, double *Q, double *R,
                   double *tmp_block, SolveState *st, const int *gate = nullptr,
-                  int *shift_flag = nullptr, int *reorth_flag = nullptr);
+                  int *shift_flag = nullptr, int *reorth_flag = nullptr, int iter_tag = -1);
 
 // Psi_i += Phi_i R1 (i < nb), C <- C2 R1: folds a re-orthogonalization of the basis block
 // into the Hessenberg column.  Gated by *gate.

@@ -71,6 +71,7 @@ __global__ void gmres_init_kernel(SolveState *st, double atol, double rtol, doub
 }
 
 __global__ void pass_begin_kernel(SolveState *st, int inner_itmax) {
+    st->qr_fail_iter = 0x7fffffff;
     st->inner_itmax = inner_itmax;
     st->inner_iter = 0;
     st->inner_tired = 0;
@@ -171,13 +172,27 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
     const int hist_cap = itmax + 2;
     double *hist = (double *)ws_get(ctx, WS_HIST, sizeof(double) * hist_cap, &s);
     if (!hist) return s;
-    // C (p x p), scratch of the factor kernel (3 p x p), C2 and fold scratch (2 p x p), tau (p)
-    double *Cm = (double *)ws_get(ctx, WS_HSCR, sizeof(double) * (6 * pp + p), &s);
-    if (!Cm) return s;
-    double *scr = Cm + pp;
-    double *C2 = Cm + 4 * pp;
-    double *fold_scr = Cm + 5 * pp;
-    double *tau_cur = Cm + 6 * pp;
+    // C blocks by iteration parity (2 p x p), C2 and fold scratch (2 p x p), tau (p), scratch of
+    // the factor kernel (3 p (p+1) + p; used for p > 64 only)
+    const size_t hscr_n = 4 * pp + p + 3 * (size_t)p * (p + 1) + p;
+    double *hscr = (double *)ws_get(ctx, WS_HSCR, sizeof(double) * hscr_n, &s);
+    if (!hscr) return s;
+    double *Cpar[2] = {hscr, hscr + pp};
+    double *C2 = hscr + 2 * pp;
+    double *fold_scr = hscr + 3 * pp;
+    double *tau_cur = hscr + 4 * pp;
+    double *scr = hscr + 4 * pp + p;
+    // The Hessenberg update of iteration k runs on the second stream, overlapped with the
+    // Arnoldi step of iteration k+1 (it feeds only the stopping test and the next update).
+    // Kernels of the main stream may then run up to two iterations past the converged one;
+    // those iterations only write basis blocks and Hessenberg columns beyond the solution's.
+    const bool overlap = ctx->overlap && ctx->hstream != nullptr;
+    int last_hess = 0;   // iteration of the last Hessenberg update enqueued on the second stream
+    auto join = [&]() -> bpf_status {   // main stream waits for the last Hessenberg update
+        if (overlap && last_hess > 0)
+            BPF_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_b[last_hess & 1], 0));
+        return BPF_SUCCESS;
+    };
     GmresBufs g{};
     // An FP32-factor right preconditioner is not exactly the same linear map at every
     // application (rounding), so the flexible form keeps the preconditioned blocks
@@ -191,6 +206,7 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
     SolveState hs;
     std::memset(&hs, 0, sizeof(hs));
     hs.itmax = itmax;
+    hs.qr_fail_iter = 0x7fffffff;
     hs.inner_itmax = itmax;
     hs.mem = memory;
     hs.restart = restart;
@@ -279,8 +295,12 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
                 BPF_TRY(tsmm(ctx, n, p, kk, g.V, np, Psi, pp, -1.0, Qk, 1.0, Qk, st));
                 BPF_TRY(gram(ctx, n, p, kk, g.V, np, Qk, Psi, 1.0, true, st, nullptr, Psi2buf));
                 BPF_TRY(tsmm(ctx, n, p, kk, g.V, np, Psi2buf, pp, -1.0, Qk, 1.0, Qk, st));
+                double *Cm = Cpar[kk & 1];
+                // Cpar[kk & 1] was last read by the Hessenberg update of iteration kk - 2
+                if (overlap && kk >= 3)
+                    BPF_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_b[kk & 1], 0));
                 BPF_TRY(cholqr(ctx, n, p, Qk, Vn, Cm, Tq, st, nullptr, &st->qr_shift,
-                               &st->qr_reorth));                             // :316
+                               &st->qr_reorth, kk));                         // :316
                 // Ill-conditioned block (Cholesky lost > 8 digits): its Q may carry amplified
                 // components along V.  Re-orthogonalize once and fold the correction into the
                 // Hessenberg column: W = V Psi + Q1 R1, Q1 = V Phi + Q2 C2
@@ -289,14 +309,28 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
                     const int *rg = &st->qr_reorth;
                     BPF_TRY(gram(ctx, n, p, kk, g.V, np, Vn, Psi2buf, 1.0, false, st, rg));
                     BPF_TRY(tsmm(ctx, n, p, kk, g.V, np, Psi2buf, pp, -1.0, Vn, 1.0, Qk, st, nullptr, rg));
-                    BPF_TRY(cholqr(ctx, n, p, Qk, Vn, C2, Tq, st, rg, &st->qr_shift2, nullptr));
+                    BPF_TRY(cholqr(ctx, n, p, Qk, Vn, C2, Tq, st, rg, &st->qr_shift2, nullptr, kk));
                     BPF_TRY(reorth_fold(ctx, p, kk, Psi, Psi2buf, Cm, C2, Cm, fold_scr, st, rg));
                 }
-                BPF_TRY(launch_hess(ctx, p, kk, g.Rblk, g.HY, tau_cur, g.Z, Cm, st, hist, scr));
+                if (overlap) {
+                    BPF_CUDA(ctx, cudaEventRecord(ctx->ev_a[kk & 1], ctx->stream));
+                    BPF_CUDA(ctx, cudaStreamWaitEvent(ctx->hstream, ctx->ev_a[kk & 1], 0));
+                    StreamSwap sw(ctx, ctx->hstream);
+                    BPF_TRY(launch_hess(ctx, p, kk, g.Rblk, g.HY, tau_cur, g.Z, Cm, st, hist, scr));
+                    BPF_CUDA(ctx, cudaEventRecord(ctx->ev_b[kk & 1], ctx->hstream));
+                    last_hess = kk;
+                } else {
+                    BPF_TRY(launch_hess(ctx, p, kk, g.Rblk, g.HY, tau_cur, g.Z, Cm, st, hist, scr));
+                }
             }
             k = kend;
+            BPF_TRY(join());
             BPF_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(SolveState), cudaMemcpyDeviceToHost, ctx->stream));
             BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            // a Cholesky-QR breakdown in an iteration that counted is an error (one in an
+            // iteration past the stopping point is not)
+            if (hs.qr_fail_iter <= hs.inner_iter)
+                return set_error(ctx, BPF_ERR_NUMERIC, "block_gmres: Cholesky-QR breakdown");
             active = hs.active != 0;
             if (opts->verbose > 0 && hs.nres > printed) {
                 int upto = std::min(hs.nres, hist_cap);

@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(512)
 chol3_kernel(int n, int p, const double *__restrict__ G, double *__restrict__ Rinv,
              double *__restrict__ Racc, double *__restrict__ gscr, int pass, SolveState *st,
              const int *gate, const int *gate2, int *shift_flag, int *reorth_flag,
-             DevStatus *ds) {
+             DevStatus *ds, int iter_tag) {
     if (st && !st->active) return;
     if (gate && *gate == 0) return;
     if (gate2 && *gate2 == 0) return;
@@ -181,6 +181,7 @@ chol3_kernel(int n, int p, const double *__restrict__ G, double *__restrict__ Ri
     double *X = SM ? rs + p : gscr;                   // p x ldx
     double *Rs = SM ? X + (size_t)p * ld : gscr + (size_t)p * p;
     __shared__ double s_trace;
+    __shared__ double s_dinv[2];               // 1 / pivot of columns j (parity j & 1)
     const int tid = threadIdx.x, nt = blockDim.x;
     const int ngrp = nt / p;                  // row groups (>= 1 for p <= nt)
     const int bcol = tid % p, grp = tid / p;
@@ -203,7 +204,7 @@ chol3_kernel(int n, int p, const double *__restrict__ G, double *__restrict__ Ri
         }
     }
     __syncthreads();
-    double minratio = 1.0;
+    bool illcond = false;   // some pivot below 1e-8 of its column's norm^2 (attempt 0)
     int fail = 0;
     for (int attempt = 0; attempt < 2; attempt++) {
         const double shift = attempt == 0 ? 0.0
@@ -215,21 +216,23 @@ chol3_kernel(int n, int p, const double *__restrict__ G, double *__restrict__ Ri
                 g[a * ld + b] = G[e] + (a == b ? shift : 0.0);
                 X[a * ldx + b] = (a == b) ? 1.0 : 0.0;
             }
-            __syncthreads();
         }
+        if (tid == 0) s_dinv[0] = 1.0 / g[0];
+        __syncthreads();
         fail = 0;
+        // first row a > j of this thread's residue class (advanced incrementally)
+        int a0 = grp;
+        if (a0 < 1) a0 += ngrp;
         for (int j = 0; j < p; j++) {
             const double d = g[j * ld + j];
             const double ref = dref[j] + shift;
-            if (attempt == 0) minratio = fmin(minratio, ref > 0.0 ? d / ref : 0.0);
+            if (attempt == 0 && !(d >= 1e-8 * ref)) illcond = true;
             if (!(d > 1e-13 * ref) || !(d > 0.0)) {
                 fail = 1;
                 break;
             }
-            const double dinv = 1.0 / d;
+            const double dinv = s_dinv[j & 1];
             if (owner) {
-                // first row a > j in this thread's residue class
-                const int a0 = j + 1 + ((grp - (j + 1)) % ngrp + ngrp) % ngrp;
                 const double *gj = g + (size_t)j * ld;
                 if (bcol > j) {
                     const double f = gj[bcol] * dinv;
@@ -246,7 +249,12 @@ chol3_kernel(int n, int p, const double *__restrict__ G, double *__restrict__ Ri
 #pragma unroll
                         for (int i = 0; i < 8; i++) {
                             const int aa = a + i * ngrp;
-                            if (aa <= bcol) g[aa * ld + bcol] = cur[i] - rj[i] * f;
+                            if (aa <= bcol) {
+                                const double nv = cur[i] - rj[i] * f;
+                                g[aa * ld + bcol] = nv;
+                                // the next pivot: its thread publishes 1 / d_{j+1}
+                                if (aa == j + 1 && bcol == j + 1) s_dinv[(j + 1) & 1] = 1.0 / nv;
+                            }
                         }
                     }
                 } else {
@@ -271,10 +279,11 @@ chol3_kernel(int n, int p, const double *__restrict__ G, double *__restrict__ Ri
                     }
                 }
             }
+            if (a0 == j + 1) a0 += ngrp;
             __syncthreads();
         }
         if (attempt == 0 && tid == 0 && pass == 0 && reorth_flag)
-            *reorth_flag = (fail || minratio < 1e-8) ? 1 : 0;
+            *reorth_flag = (fail || illcond) ? 1 : 0;
         if (!fail) break;
         if (tid == 0 && shift_flag) *shift_flag = 1;
         __syncthreads();
@@ -282,7 +291,10 @@ chol3_kernel(int n, int p, const double *__restrict__ G, double *__restrict__ Ri
     if (fail) {
         if (tid == 0) {
             if (st) st->qr_fail = 1;
-            if (ds && atomicCAS(&ds->err, 0, (int)DEV_CHOL_FAIL) == 0) ds->aux = pass;
+            if (iter_tag >= 0 && st)
+                atomicMin(&st->qr_fail_iter, iter_tag);
+            else if (ds && atomicCAS(&ds->err, 0, (int)DEV_CHOL_FAIL) == 0)
+                ds->aux = pass;
         }
         return;
     }
@@ -319,7 +331,7 @@ chol3_kernel(int n, int p, const double *__restrict__ G, double *__restrict__ Ri
 
 bpf_status launch_chol(bpf_ctx *ctx, int n, int p, const double *G, double *Rinv, double *Racc,
                        double *gscr, int pass, SolveState *st, const int *gate, const int *gate2,
-                       int *shift_flag, int *reorth_flag) {
+                       int *shift_flag, int *reorth_flag, int iter_tag) {
     const int nt = p > 32 ? 512 : 256;
     const size_t one = sizeof(double) * p * (p + 1);
     const size_t extra = sizeof(double) * 2 * p;
@@ -331,13 +343,13 @@ bpf_status launch_chol(bpf_ctx *ctx, int n, int p, const double *G, double *Rinv
             BPF_CUDA(ctx, cudaFuncSetAttribute(chol3_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)smem));
         chol3_kernel<true><<<1, nt, smem, ctx->stream>>>(n, p, G, Rinv, Racc, gscr, pass, st, gate, gate2,
-                                                         shift_flag, reorth_flag, ctx->dstat);
+                                                         shift_flag, reorth_flag, ctx->dstat, iter_tag);
     } else {
         if (smem > 48 * 1024)
             BPF_CUDA(ctx, cudaFuncSetAttribute(chol3_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)smem));
         chol3_kernel<false><<<1, nt, smem, ctx->stream>>>(n, p, G, Rinv, Racc, gscr, pass, st, gate, gate2,
-                                                          shift_flag, reorth_flag, ctx->dstat);
+                                                          shift_flag, reorth_flag, ctx->dstat, iter_tag);
     }
     BPF_LAUNCHED(ctx);
     return BPF_SUCCESS;
@@ -533,7 +545,7 @@ hess_factor3_kernel(int p, int k, double *__restrict__ Rblk, double *__restrict_
         X = scr + (size_t)2 * p * ld;
     }
     __shared__ double red[32];
-    __shared__ double s_xn2;
+    __shared__ double s_refl[3];   // tau, 1 / (alpha - beta), beta of the current column
     __shared__ int s_anyzero;
     for (int e = tid; e < p * p; e += nt) {
         const int a = e / p, b = e - a * p;
@@ -568,24 +580,25 @@ hess_factor3_kernel(int p, int k, double *__restrict__ Rblk, double *__restrict_
             d = s0 + s1;
         }
         for (int o = 1; o < G; o <<= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
-        if (owner && c2 == c && grp == 0) s_xn2 = d;
+        // the reflector scalars, once, by the lane that owns (c, row group 0)
+        if (owner && c2 == c && grp == 0) {
+            const double alpha = F[c * ld + c];
+            const double xn = sqrt(d);
+            double tc0 = 0.0, sc0 = 0.0, beta0 = alpha;
+            if (xn != 0.0) {
+                beta0 = -copysign(hypot(alpha, xn), alpha);
+                tc0 = (beta0 - alpha) / beta0;
+                sc0 = 1.0 / (alpha - beta0);
+            } else {
+                s_anyzero = 1;
+            }
+            s_refl[0] = tc0;
+            s_refl[1] = sc0;
+            s_refl[2] = beta0;
+            tau[c] = tc0;
+        }
         __syncthreads();
-        const double alpha = F[c * ld + c];
-        const double xn = sqrt(s_xn2);
-        double tc, sc, beta;
-        if (xn == 0.0) {
-            tc = 0.0;
-            sc = 0.0;
-            beta = alpha;
-        } else {
-            beta = -copysign(hypot(alpha, xn), alpha);
-            tc = (beta - alpha) / beta;
-            sc = 1.0 / (alpha - beta);
-        }
-        if (tid == 0) {
-            tau[c] = tc;
-            if (xn == 0.0) s_anyzero = 1;
-        }
+        const double tc = s_refl[0], sc = s_refl[1], beta = s_refl[2];
         if (tc != 0.0 && owner && c2 > c) {
             const double w = tc * (fcc2 + sc * d);
             const double wsc = w * sc;
@@ -724,7 +737,7 @@ bpf_status launch_hess(bpf_ctx *ctx, int p, int k, double *Rblk, double *HY, dou
         hess_apply4_kernel<false><<<ncb, 256, small_a, ctx->stream>>>(p, k, Rblk, HY, st, ctx->dstat);
     }
     BPF_LAUNCHED(ctx);
-    const int nt = p > 32 ? 512 : 256;
+    const int nt = p > 64 ? 512 : 256;
     const size_t base_f = sizeof(double) * (2 * (size_t)p);
     const size_t smem_f = base_f + sizeof(double) * 6 * (size_t)p * factor_ld(p, true);
     if (smem_f <= 220 * 1024) {

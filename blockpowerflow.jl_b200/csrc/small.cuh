@@ -21,7 +21,7 @@ __host__ __device__ inline size_t hy_stride(int p) {
 // gscr: 2 p^2 doubles of global scratch.  Flags as documented at cholqr().
 bpf_status launch_chol(bpf_ctx *ctx, int n, int p, const double *G, double *Rinv, double *Racc,
                        double *gscr, int pass, SolveState *st, const int *gate, const int *gate2,
-                       int *shift_flag, int *reorth_flag);
+                       int *shift_flag, int *reorth_flag, int iter_tag = -1);
 
 // One block-Hessenberg QR update of block-GMRES iteration k (1-based): apply the stored
 // reflectors to block column k-1, factor [R_jj; C], update Z and the stopping test.
