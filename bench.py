@@ -42,6 +42,9 @@ N_BUS, N_PV, P_RHS = 9000, 1000, 64
 RTOL = 1e-8
 ITMAX = 300
 CPU_SAMPLE_ITERS = (4, 10)
+# DRAM bytes (read + write) per launch of each kernel class, from one ncu capture of the
+# benchmark's solve (profiles/launches_grid9k_p64.md); None where not captured.
+TRAFFIC_PER_LAUNCH = {}
 
 
 def peaks():
@@ -51,6 +54,29 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def fp64_peak_tflops(device):
+    """FP64 tensor-pipe reference: cuBLAS DGEMM (torch.matmul, float64, 8192^3), best of 5
+    after 2 warm-up products, CUDA events.  The peaks file has no FP64 figure."""
+    import torch
+
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
 
 
 class ClockSampler:
@@ -174,7 +200,7 @@ def workload_config(world):
             "parallelism": f"replicas x{world} (independent grids)"}
 
 
-def kernel_only(name, reps):
+def kernel_only(name, reps, iters=24):
     """A few launches of one kernel on a case whose blocks exceed L2, for ncu captures:
     70,000-bus grid (134,998 unknowns, ~980k nonzeros), 128 right-hand sides."""
     import numpy as np
@@ -183,15 +209,15 @@ def kernel_only(name, reps):
     import blockpowerflow_b200 as bpf
 
     if name == "gmres":
-        # 24 iterations of the benchmark's solve (9,000-bus grid, 64 RHS): every kernel of the
-        # block-GMRES iteration, for a launch list
+        # `iters` iterations of the benchmark's solve (9,000-bus grid, 64 RHS; 69 = the whole
+        # solve): every kernel of the block-GMRES iteration, for a launch list
         J, B = make_workload(0)
         A = bpf.CuSparseMatrixCSR.from_scipy(J)
         Bd = bpf.colmajor(torch.as_tensor(B, device="cuda"))
         N = bpf.ilu0(A, P_RHS)
         for _ in range(reps):
             X, st = bpf.block_gmres(A, Bd, N=N, ldiv=True, restart=False, memory=ITMAX, atol=0.0,
-                                    rtol=RTOL, itmax=24)
+                                    rtol=RTOL, itmax=iters)
         torch.cuda.synchronize()
         print(json.dumps({"kernel_only": name, "n": J.shape[0], "p": P_RHS, "reps": reps,
                           "iterations": st.niter}))
@@ -222,6 +248,7 @@ def main():
     ap.add_argument("--kernel-only", choices=["trsv", "spmm", "factor", "gram", "gmres"], default=None,
                     help="launch one kernel a few times on a 135k-unknown case (for ncu)")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--iters", type=int, default=24, help="block-GMRES iterations (--kernel-only gmres)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -231,7 +258,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.kernel_only:
-        kernel_only(args.kernel_only, args.reps)
+        kernel_only(args.kernel_only, args.reps, args.iters)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -365,7 +392,6 @@ def main():
     # ---- roofline of the dominant kernel class -------------------------------------------
     hbm, hbm_src = peaks()
     kern, t_ms = r["kern"], r["t_ms"]
-    dom = max(kern, key=lambda k: kern[k]["ms"])
     breakdown = {}
     for k, v in kern.items():
         if v["launches"] == 0:
@@ -375,17 +401,35 @@ def main():
                         "avg_us": 1e3 * v["ms"] / v["launches"],
                         "GBps": v["bytes"] / s / 1e9 if v["bytes"] else None,
                         "TFLOPs": v["flops"] / s / 1e12 if v["flops"] else None}
-    # HBM-bound classes are the sparse kernels; Gram / tsmm run on the FP64 pipe at p = 64.
-    hbm_classes = ("trsv", "spmm", "factor")
-    rk = dom if dom in hbm_classes else max(hbm_classes, key=lambda k: kern[k]["ms"])
-    v = kern[rk]
-    ach = v["bytes"] / (v["ms"] / 1e3) / 1e9 if v["ms"] > 0 else 0.0
-    roofline = {"bound": "hbm", "kernel": rk, "achieved": ach, "peak": hbm, "unit": "GB/s",
-                "frac": ach / hbm, "peak_source": hbm_src,
-                "bytes_per_launch": v["bytes"] / max(v["launches"], 1),
-                "avg_launch_us": 1e3 * v["ms"] / max(v["launches"], 1),
-                "traffic": None, "dominant_class": dom,
-                "dominant_share_of_device_time": kern[dom]["ms"] / max(t_ms, 1e-9)}
+    # The Hessenberg class runs on the second stream, overlapped with the Arnoldi step, so
+    # the dominant class is taken among the main-stream classes.
+    main = [k for k in kern if k != "hess"]
+    dom = max(main, key=lambda k: kern[k]["ms"])
+    fp64_peak = fp64_peak_tflops(dev)
+    v = kern[dom]
+    secs = v["ms"] / 1e3 if v["ms"] > 0 else float("inf")
+    if dom in ("gram", "tsmm"):
+        ach = v["flops"] / secs / 1e12
+        roofline = {"bound": "tensor", "kernel": dom, "achieved": ach, "peak": fp64_peak,
+                    "unit": "TFLOP/s", "frac": ach / fp64_peak,
+                    "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64 tensor pipe)",
+                    "flops_per_launch": v["flops"] / max(v["launches"], 1),
+                    "bytes_per_launch": v["bytes"] / max(v["launches"], 1)}
+    else:
+        ach = v["bytes"] / secs / 1e9
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
+                    "frac": ach / hbm, "peak_source": hbm_src,
+                    "bytes_per_launch": v["bytes"] / max(v["launches"], 1)}
+    roofline.update({"avg_launch_us": 1e3 * v["ms"] / max(v["launches"], 1),
+                     "traffic": TRAFFIC_PER_LAUNCH.get(dom),
+                     "dominant_share_of_device_time": v["ms"] / max(t_ms, 1e-9)})
+    # the HBM-bound sparse kernels beside it (triangular solves, SpMM)
+    sparse = {}
+    for k in ("trsv", "spmm"):
+        w = kern[k]
+        if w["ms"] > 0:
+            a = w["bytes"] / (w["ms"] / 1e3) / 1e9
+            sparse[k] = {"achieved_GBps": a, "frac_of_hbm": a / hbm, "peak_source": hbm_src}
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(J, B, results["fp64"]["iterations"], os.cpu_count() or 1)
@@ -405,7 +449,8 @@ def main():
         "e2e": {"value": e2e_val, "unit": UNIT,
                 "h2d_bytes_per_step": int(8 * (J.nnz + n * P_RHS)),
                 "d2h_bytes_per_step": int(8 * n * P_RHS)},
-        "gpu_launches": r["launches"], "roofline": roofline, "kernels": breakdown,
+        "gpu_launches": r["launches"], "roofline": roofline, "roofline_sparse": sparse,
+        "kernels": breakdown,
         "cpu_baseline": cb, "clocks": clocks,
     }
     if rank == 0:

@@ -123,16 +123,19 @@ bpf_status reset_dev_status(bpf_ctx *ctx);
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
-// Records a CUDA event pair around one launch when the context's timing is on.
+// Records a CUDA event pair around one launch when the context's timing is on.  A launch
+// gated on a device flag (it returns at once unless a rare condition was raised) is not
+// recorded (gated = true): its algorithmic bytes and flops would count work it skips, so the
+// class totals cover the launches that always do their work.
 cudaEvent_t timing_event(bpf_ctx *ctx);
 struct KScope {
     bpf_ctx *ctx;
     int kc;
     double bytes, flops;
     cudaEvent_t a = nullptr;
-    KScope(bpf_ctx *c, int k, double algo_bytes = 0.0, double algo_flops = 0.0)
+    KScope(bpf_ctx *c, int k, double algo_bytes = 0.0, double algo_flops = 0.0, bool gated = false)
         : ctx(c), kc(k), bytes(algo_bytes), flops(algo_flops) {
-        if (ctx->timing) {
+        if (ctx->timing && !gated) {
             a = timing_event(ctx);
             if (a) cudaEventRecord(a, ctx->stream);
         }

@@ -114,6 +114,12 @@ __global__ void gram_dmma_cl_kernel(int n, int p, int nb, const double *__restri
                                     size_t strideA, const double *__restrict__ B,
                                     double *__restrict__ partial, int rows_per_chunk,
                                     const SolveState *st, const int *gate, const int *gate2);
+__global__ void
+gram_pipe_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
+                 const double *__restrict__ B, double *__restrict__ partial, int rows_per_chunk,
+                 const SolveState *st, const int *gate, const int *gate2);
+static bool pipe_ok(int p, const void *A, size_t strideA, const void *B, size_t strideB);
+extern const size_t kGramPipeSmemBytes;
 
 bpf_status gram(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t strideA,
                 const double *B, double *Out, double alpha, bool accumulate,
@@ -137,8 +143,14 @@ bpf_status gram(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
     double *partial = (double *)ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)nparts * nb * p * p, &s);
     if (!partial) return s;
     dim3 grid(grid_x, nb, tiles);
-    KScope ks(ctx, BPF_KC_GRAM, 8.0 * n * p * (nb + (A == B ? 0 : 1)), 2.0 * n * p * (double)p * nb);
-    if (cl) {
+    KScope ks(ctx, BPF_KC_GRAM, 8.0 * n * p * (nb + (A == B ? 0 : 1)), 2.0 * n * p * (double)p * nb,
+              qr_gate != nullptr || gate2 != nullptr);
+    if (cl && GT == 64 && pipe_ok(p, A, strideA, B, 0)) {
+        BPF_CUDA(ctx, cudaFuncSetAttribute(gram_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kGramPipeSmemBytes));
+        gram_pipe_kernel<<<grid, 256, kGramPipeSmemBytes, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
+                                                                         rows_per_chunk, st, qr_gate, gate2);
+    } else if (cl) {
         if (GT == 16)
             gram_dmma_cl_kernel<16><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
                                                                     rows_per_chunk, st, qr_gate, gate2);
@@ -387,6 +399,220 @@ tsmm_dmma_kernel(int n, int p, int nb, const double *__restrict__ A, size_t stri
 }
 
 // ---------------------------------------------------------------------------------------
+// Pipelined FP64 tensor-core products (p even, 32 < p, 64-wide output tiles): 8 warps in a
+// 4 x 2 layout (16 x 32 outputs each), operands staged by 16-byte cp.async in a 3-stage ring
+// so the loads of chunk c+2 are in flight while chunk c computes; padded row strides (36 and
+// 68 doubles) keep the m8n8k4 fragment loads free of bank conflicts.  ~105 KB of shared
+// memory per CTA, two CTAs per SM.
+// ---------------------------------------------------------------------------------------
+constexpr int kPipeStages = 3;
+
+__device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, int src_bytes) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Out (rows r0..r0+63, columns b0..b0+63) = beta*Cin + alpha*sum_j A_j S_j.
+__global__ void __launch_bounds__(256, 2)
+tsmm_pipe_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
+                 const double *__restrict__ S, size_t strideS, double alpha, const double *Cin,
+                 double beta, double *Out, const SolveState *st, const int *gate, const int *gate2) {
+    if (gate_off(st, gate, gate2)) return;
+    constexpr int BM = 64, GT = 64, KC = 32, SA = KC + 4, SB = GT + 4, ST = kPipeStages;
+    extern __shared__ __align__(16) double psm[];
+    double *As = psm;                          // ST x BM x SA
+    double *Bs = psm + ST * BM * SA;           // ST x KC x SB
+    const int r0 = blockIdx.x * BM, b0 = blockIdx.y * GT;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t4 = lane & 3;
+    const int kpb = (p + KC - 1) / KC;
+    const int nchunks = nb * kpb;
+    auto load = [&](int ch, int stage) {
+        const int j = ch / kpb, k0 = (ch - j * kpb) * KC;
+        const double *Aj = A + (size_t)j * strideA;
+        const double *Sj = S + (size_t)j * strideS;
+        double *as = As + stage * BM * SA;
+        double *bs = Bs + stage * KC * SB;
+#pragma unroll
+        for (int q = 0; q < BM * KC / 2 / 256; q++) {
+            const int e = tid + q * 256;
+            const int rr = e / (KC / 2), cc = (e % (KC / 2)) * 2;
+            const int r = r0 + rr, c = k0 + cc;
+            const bool ok = r < n && c < p;
+            cp_async16_zfill(as + rr * SA + cc, ok ? Aj + (size_t)r * p + c : Aj, ok ? 16 : 0);
+        }
+#pragma unroll
+        for (int q = 0; q < KC * GT / 2 / 256; q++) {
+            const int e = tid + q * 256;
+            const int kk = e / (GT / 2), cc = (e % (GT / 2)) * 2;
+            const int a = k0 + kk, b = b0 + cc;
+            const bool ok = a < p && b < p;
+            cp_async16_zfill(bs + kk * SB + cc, ok ? Sj + (size_t)a * p + b : Sj, ok ? 16 : 0);
+        }
+    };
+    double acc[2][4][2];
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int ni = 0; ni < 4; ni++) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+#pragma unroll
+    for (int s0 = 0; s0 < ST - 1; s0++) {
+        if (s0 < nchunks) load(s0, s0);
+        cp_async_commit_group();
+    }
+    for (int ch = 0; ch < nchunks; ch++) {
+        cp_async_wait_group<ST - 2>();
+        __syncthreads();
+        const int nxt = ch + ST - 1;   // its stage was consumed at iteration ch - 1
+        if (nxt < nchunks) load(nxt, nxt % ST);
+        cp_async_commit_group();
+        const double *as = As + (ch % ST) * BM * SA;
+        const double *bs = Bs + (ch % ST) * KC * SB;
+#pragma unroll
+        for (int ks = 0; ks < KC / 4; ks++) {
+            const int k = ks * 4 + t4;
+            double a[2], b[4];
+#pragma unroll
+            for (int mi = 0; mi < 2; mi++) a[mi] = as[(wm * 16 + mi * 8 + g) * SA + k];
+#pragma unroll
+            for (int ni = 0; ni < 4; ni++) b[ni] = bs[k * SB + wn * 32 + ni * 8 + g];
+#pragma unroll
+            for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+                for (int ni = 0; ni < 4; ni++) dmma884(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+        }
+    }
+    cp_async_wait_group<0>();
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++) {
+        const int r = r0 + wm * 16 + mi * 8 + g;
+        if (r >= n) continue;
+#pragma unroll
+        for (int ni = 0; ni < 4; ni++) {
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                const int b = b0 + wn * 32 + ni * 8 + 2 * t4 + i;
+                if (b >= p) continue;
+                double v = alpha * acc[mi][ni][i];
+                if (Cin && beta != 0.0) v += beta * Cin[(size_t)r * p + b];
+                Out[(size_t)r * p + b] = v;
+            }
+        }
+    }
+}
+
+// Partial Gram tile (a0.., b0..) of A_j^T B over one chunk of rows; chunks grouped in clusters
+// of 8 CTAs whose partial tiles are summed through distributed shared memory (one partial per
+// cluster goes to global memory).  The gate is uniform across a cluster.
+__global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256)
+gram_pipe_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
+                 const double *__restrict__ B, double *__restrict__ partial, int rows_per_chunk,
+                 const SolveState *st, const int *gate, const int *gate2) {
+    if (gate_off(st, gate, gate2)) return;
+    namespace cg = cooperative_groups;
+    constexpr int GT = 64, RS = 32, SB = GT + 4, ST = kPipeStages;
+    extern __shared__ __align__(16) double psm[];
+    double *As = psm;                          // ST x RS x SB
+    double *Bs = psm + ST * RS * SB;           // ST x RS x SB
+    const int chunk = blockIdx.x, j = blockIdx.y;
+    const int ntile = (p + GT - 1) / GT;
+    const int a0 = (blockIdx.z / ntile) * GT, b0 = (blockIdx.z % ntile) * GT;
+    const int r_begin = chunk * rows_per_chunk;
+    const int r_end = min(n, r_begin + rows_per_chunk);
+    const int nst = r_end > r_begin ? (r_end - r_begin + RS - 1) / RS : 0;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t4 = lane & 3;
+    const double *Aj = A + (size_t)j * strideA;
+    auto load = [&](int sidx, int stage) {
+        const int rb = r_begin + sidx * RS;
+        double *as = As + stage * RS * SB;
+        double *bs = Bs + stage * RS * SB;
+#pragma unroll
+        for (int q = 0; q < RS * GT / 2 / 256; q++) {
+            const int e = tid + q * 256;
+            const int rr = e / (GT / 2), cc = (e % (GT / 2)) * 2;
+            const int r = rb + rr;
+            const bool rok = r < r_end;
+            const bool oka = rok && a0 + cc < p, okb = rok && b0 + cc < p;
+            cp_async16_zfill(as + rr * SB + cc, oka ? Aj + (size_t)r * p + a0 + cc : Aj, oka ? 16 : 0);
+            cp_async16_zfill(bs + rr * SB + cc, okb ? B + (size_t)r * p + b0 + cc : B, okb ? 16 : 0);
+        }
+    };
+    double acc[2][4][2];
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int ni = 0; ni < 4; ni++) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+#pragma unroll
+    for (int s0 = 0; s0 < ST - 1; s0++) {
+        if (s0 < nst) load(s0, s0);
+        cp_async_commit_group();
+    }
+    for (int sidx = 0; sidx < nst; sidx++) {
+        cp_async_wait_group<ST - 2>();
+        __syncthreads();
+        const int nxt = sidx + ST - 1;
+        if (nxt < nst) load(nxt, nxt % ST);
+        cp_async_commit_group();
+        const double *as = As + (sidx % ST) * RS * SB;
+        const double *bs = Bs + (sidx % ST) * RS * SB;
+#pragma unroll
+        for (int ks = 0; ks < RS / 4; ks++) {
+            const int k = ks * 4 + t4;
+            double a[2], b[4];
+#pragma unroll
+            for (int mi = 0; mi < 2; mi++) a[mi] = as[k * SB + wm * 16 + mi * 8 + g];
+#pragma unroll
+            for (int ni = 0; ni < 4; ni++) b[ni] = bs[k * SB + wn * 32 + ni * 8 + g];
+#pragma unroll
+            for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+                for (int ni = 0; ni < 4; ni++) dmma884(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+        }
+    }
+    cp_async_wait_group<0>();
+    __syncthreads();
+    // this CTA's tile into its shared memory (GT x GT, row-major), then the cluster sum
+    double *tile = psm;
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int ni = 0; ni < 4; ni++)
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+                tile[(wm * 16 + mi * 8 + g) * GT + wn * 32 + ni * 8 + 2 * t4 + i] = acc[mi][ni][i];
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();
+    const int rank = (int)cluster.block_rank();
+    constexpr int RPR = GT / 8;
+    double *out = partial + ((size_t)(chunk / 8) * nb + j) * p * p;
+    for (int e = tid; e < RPR * GT; e += 256) {
+        const int a = rank * RPR + e / GT, b = e % GT;
+        double sum = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) sum += cluster.map_shared_rank(tile, q)[a * GT + b];
+        if (a0 + a < p && b0 + b < p) out[(size_t)(a0 + a) * p + b0 + b] = sum;
+    }
+    cluster.sync();
+}
+
+// True when the pipelined kernels apply: 16-byte aligned rows (p even, aligned bases and
+// strides) and 64-wide tiles.
+static bool pipe_ok(int p, const void *A, size_t strideA, const void *B, size_t strideB) {
+    if (p <= 32 || (p & 1)) return false;
+    if (((uintptr_t)A | (uintptr_t)B) & 15) return false;
+    if ((strideA | strideB) & 1) return false;
+    return true;
+}
+constexpr size_t kTsmmPipeSmem = sizeof(double) * kPipeStages * (64 * 36 + 32 * 68);
+constexpr size_t kGramPipeSmem = sizeof(double) * kPipeStages * 2 * 32 * 68;
+extern const size_t kGramPipeSmemBytes = kGramPipeSmem;
+
+// ---------------------------------------------------------------------------------------
 // tsmm
 // ---------------------------------------------------------------------------------------
 template <int GT>
@@ -463,8 +689,13 @@ bpf_status tsmm(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
     const int GT = p <= 16 ? 16 : (p <= 32 ? 32 : 64);
     dim3 grid(ceil_div(n, kTsmmRows), ceil_div(p, GT));
     KScope ks(ctx, BPF_KC_TSMM, 8.0 * n * p * (nb + 1 + ((Cin && beta != 0.0) ? 1 : 0)),
-              2.0 * n * p * (double)p * nb);
-    if (ctx->fp64_mma) {
+              2.0 * n * p * (double)p * nb, qr_gate != nullptr || gate2 != nullptr || nb_dev != nullptr);
+    if (ctx->fp64_mma && GT == 64 && !nb_dev && pipe_ok(p, A, strideA, S, strideS)) {
+        BPF_CUDA(ctx, cudaFuncSetAttribute(tsmm_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kTsmmPipeSmem));
+        tsmm_pipe_kernel<<<grid, 256, kTsmmPipeSmem, ctx->stream>>>(n, p, nb, A, strideA, S, strideS, alpha,
+                                                                    Cin, beta, Out, st, qr_gate, gate2);
+    } else if (ctx->fp64_mma) {
         if (GT == 16)
             tsmm_dmma_kernel<16><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, S, strideS, alpha,
                                                                  Cin, beta, Out, st, nb_dev, qr_gate, gate2);

@@ -337,7 +337,7 @@ bpf_status launch_chol(bpf_ctx *ctx, int n, int p, const double *G, double *Rinv
     const size_t extra = sizeof(double) * 2 * p;
     const bool sm = 3 * one + extra <= 200 * 1024;
     const size_t smem = (sm ? 3 * one : one) + extra;
-    KScope ks(ctx, BPF_KC_CHOL);
+    KScope ks(ctx, BPF_KC_CHOL, 0.0, 0.0, gate != nullptr || gate2 != nullptr);
     if (sm) {
         if (smem > 48 * 1024)
             BPF_CUDA(ctx, cudaFuncSetAttribute(chol3_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
