@@ -114,10 +114,19 @@ __global__ void gram_dmma_cl_kernel(int n, int p, int nb, const double *__restri
                                     size_t strideA, const double *__restrict__ B,
                                     double *__restrict__ partial, int rows_per_chunk,
                                     const SolveState *st, const int *gate, const int *gate2);
+// Epilogue of gram_pipe_kernel when the row chunks of a block form a single cluster: the
+// cluster's sum is the result (Out = alpha * sum [+ Out], Out2 = alpha * sum).
+struct GramEpilogue {
+    int direct;
+    int accumulate;
+    double alpha;
+    double *out;
+    double *out2;
+};
 __global__ void
 gram_pipe_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
                  const double *__restrict__ B, double *__restrict__ partial, int rows_per_chunk,
-                 const SolveState *st, const int *gate, const int *gate2);
+                 const SolveState *st, const int *gate, const int *gate2, GramEpilogue ep);
 static bool pipe_ok(int p, const void *A, size_t strideA, const void *B, size_t strideB);
 extern const size_t kGramPipeSmemBytes;
 
@@ -128,6 +137,55 @@ bpf_status gram(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
     const int GT = p <= 16 ? 16 : (p <= 32 ? 32 : 64);
     const int ntile = ceil_div(p, GT);
     const int tiles = ntile * ntile;
+    bpf_status s;
+    if (ctx->fp64_mma && GT == 64 && pipe_ok(p, A, strideA, B, 0)) {
+        // One wave of resident CTAs (two per SM): the cluster size cs and the number of
+        // clusters per block are picked so that cs * ncl * nb * tiles fits it, with at least
+        // 128 rows per CTA; a block covered by one cluster skips the partial-sum pass.
+        const int slots = 2 * ctx->num_sms;
+        const int units = nb * tiles;
+        int cs = 8;
+        while (cs > 1 && cs * units > slots) cs >>= 1;
+        int ncl = std::max(1, slots / (cs * units));
+        ncl = std::max(1, std::min(ncl, n / (cs * 128)));
+        const int pchunks = cs * ncl;
+        int rpc = ceil_div(std::max(n, 1), pchunks);
+        rpc = ceil_div(rpc, 32) * 32;
+        const bool direct = ncl == 1;
+        double *part2 = nullptr;
+        if (!direct) {
+            part2 = (double *)ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)ncl * nb * p * p, &s);
+            if (!part2) return s;
+        }
+        KScope ks(ctx, BPF_KC_GRAM, 8.0 * n * p * (nb + (A == B ? 0 : 1)), 2.0 * n * p * (double)p * nb,
+                  qr_gate != nullptr || gate2 != nullptr);
+        BPF_CUDA(ctx, cudaFuncSetAttribute(gram_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kGramPipeSmemBytes));
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(pchunks, nb, tiles);
+        cfg.blockDim = dim3(256, 1, 1);
+        cfg.dynamicSmemBytes = kGramPipeSmemBytes;
+        cfg.stream = ctx->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cs;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        GramEpilogue ep{direct ? 1 : 0, accumulate ? 1 : 0, alpha, Out, Out2};
+        BPF_CUDA(ctx, cudaLaunchKernelEx(&cfg, gram_pipe_kernel, n, p, nb, A, strideA, B, part2, rpc,
+                                         st, qr_gate, gate2, ep));
+        BPF_LAUNCHED(ctx);
+        if (!direct) {
+            const int total = nb * p * p;
+            const int blocks = std::min(ceil_div(total, 256), ctx->num_sms * 4);
+            gram_reduce_kernel<<<blocks, 256, 0, ctx->stream>>>(total, ncl, part2, Out, alpha,
+                                                                 accumulate ? 1 : 0, Out2, st, qr_gate, gate2);
+            BPF_LAUNCHED(ctx);
+        }
+        return BPF_SUCCESS;
+    }
     const int target = ctx->num_sms * 4;
     int nchunks = std::max(1, std::min(ceil_div(n, kGramRows), target / std::max(1, nb * tiles)));
     int rows_per_chunk = ceil_div(std::max(n, 1), nchunks);
@@ -139,18 +197,12 @@ bpf_status gram(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
     const int nclusters = ceil_div(nchunks, 8);
     const int grid_x = cl ? 8 * nclusters : nchunks;
     const int nparts = cl ? nclusters : nchunks;
-    bpf_status s;
     double *partial = (double *)ws_get(ctx, WS_PARTIAL, sizeof(double) * (size_t)nparts * nb * p * p, &s);
     if (!partial) return s;
     dim3 grid(grid_x, nb, tiles);
     KScope ks(ctx, BPF_KC_GRAM, 8.0 * n * p * (nb + (A == B ? 0 : 1)), 2.0 * n * p * (double)p * nb,
               qr_gate != nullptr || gate2 != nullptr);
-    if (cl && GT == 64 && pipe_ok(p, A, strideA, B, 0)) {
-        BPF_CUDA(ctx, cudaFuncSetAttribute(gram_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)kGramPipeSmemBytes));
-        gram_pipe_kernel<<<grid, 256, kGramPipeSmemBytes, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
-                                                                         rows_per_chunk, st, qr_gate, gate2);
-    } else if (cl) {
+    if (cl) {
         if (GT == 16)
             gram_dmma_cl_kernel<16><<<grid, 128, 0, ctx->stream>>>(n, p, nb, A, strideA, B, partial,
                                                                     rows_per_chunk, st, qr_gate, gate2);
@@ -508,10 +560,10 @@ tsmm_pipe_kernel(int n, int p, int nb, const double *__restrict__ A, size_t stri
 // Partial Gram tile (a0.., b0..) of A_j^T B over one chunk of rows; chunks grouped in clusters
 // of 8 CTAs whose partial tiles are summed through distributed shared memory (one partial per
 // cluster goes to global memory).  The gate is uniform across a cluster.
-__global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256)
+__global__ void __launch_bounds__(256)
 gram_pipe_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
                  const double *__restrict__ B, double *__restrict__ partial, int rows_per_chunk,
-                 const SolveState *st, const int *gate, const int *gate2) {
+                 const SolveState *st, const int *gate, const int *gate2, GramEpilogue ep) {
     if (gate_off(st, gate, gate2)) return;
     namespace cg = cooperative_groups;
     constexpr int GT = 64, RS = 32, SB = GT + 4, ST = kPipeStages;
@@ -587,15 +639,26 @@ gram_pipe_kernel(int n, int p, int nb, const double *__restrict__ A, size_t stri
                 tile[(wm * 16 + mi * 8 + g) * GT + wn * 32 + ni * 8 + 2 * t4 + i] = acc[mi][ni][i];
     cg::cluster_group cluster = cg::this_cluster();
     cluster.sync();
+    const int cs = (int)cluster.num_blocks();
     const int rank = (int)cluster.block_rank();
-    constexpr int RPR = GT / 8;
-    double *out = partial + ((size_t)(chunk / 8) * nb + j) * p * p;
-    for (int e = tid; e < RPR * GT; e += 256) {
-        const int a = rank * RPR + e / GT, b = e % GT;
+    const int rpr = GT / cs;   // tile rows summed by each CTA of the cluster
+    const size_t pp = (size_t)p * p;
+    double *out = partial + ((size_t)(chunk / cs) * nb + j) * pp;
+    for (int e = tid; e < rpr * GT; e += 256) {
+        const int a = rank * rpr + e / GT, b = e % GT;
         double sum = 0.0;
-#pragma unroll
-        for (int q = 0; q < 8; q++) sum += cluster.map_shared_rank(tile, q)[a * GT + b];
-        if (a0 + a < p && b0 + b < p) out[(size_t)(a0 + a) * p + b0 + b] = sum;
+        for (int q = 0; q < cs; q++) sum += cluster.map_shared_rank(tile, q)[a * GT + b];
+        if (a0 + a < p && b0 + b < p) {
+            const size_t idx = (size_t)(a0 + a) * p + b0 + b;
+            if (ep.direct) {   // one cluster per block: the final result, as the reduce kernel
+                double v = ep.alpha * sum;
+                if (ep.out2) ep.out2[(size_t)j * pp + idx] = v;
+                if (ep.accumulate) v += ep.out[(size_t)j * pp + idx];
+                ep.out[(size_t)j * pp + idx] = v;
+            } else {
+                out[idx] = sum;
+            }
+        }
     }
     cluster.sync();
 }
