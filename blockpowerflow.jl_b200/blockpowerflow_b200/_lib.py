@@ -84,6 +84,9 @@ SIGNATURES = {
     "bpf_householder": (_I, [_P, _I, _I, _P, _I, _P, _I]),
     "bpf_ilu0_create": (_I, [_P, C.POINTER(CsrDesc), _I, _I, C.POINTER(_P)]),
     "bpf_ic0_create": (_I, [_P, C.POINTER(CsrDesc), _I, _I, C.POINTER(_P)]),
+    "bpf_ilu0_create_ordered": (_I, [_P, C.POINTER(CsrDesc), _I, _I, _I, C.POINTER(_P)]),
+    "bpf_ic0_create_ordered": (_I, [_P, C.POINTER(CsrDesc), _I, _I, _I, C.POINTER(_P)]),
+    "bpf_prec_permutation": (_I, [_P, _P]),
     "bpf_prec_refactor": (_I, [_P, _P]),
     "bpf_prec_apply": (_I, [_P, _I, _P, _I, _P, _I]),
     "bpf_prec_apply_noalloc": (_I, [_P, _I, _P, _I, _P, _I]),

@@ -10,19 +10,37 @@ from .sparse import CuSparseMatrixCSR, colmajor, empty_colmajor, ld
 class _DevicePrec:
     kind = ""
 
-    def __init__(self, A: CuSparseMatrixCSR, nrhs: int, factor_dtype: str, creator: str):
+    def __init__(self, A: CuSparseMatrixCSR, nrhs: int, factor_dtype: str, creator: str,
+                 ordering: str = "natural"):
         self.A = A
         self.n = A.n
         self.nrhs = int(nrhs)
         self.factor_dtype = factor_dtype
         fd = _lib.BPF_F32 if factor_dtype in ("float32", "f32", "Float32") else _lib.BPF_F64
+        key = ordering.lstrip(":").upper() if isinstance(ordering, str) else ordering
+        if key not in _lib.ORDERINGS:
+            raise ValueError(f"unknown ordering {ordering!r}")
+        self.ordering = key
         lib = _lib.load()
         self._ctx = _lib.context(A.nzVal.device.index)
         h = C.c_void_p()
         d = A.desc()
-        _lib.check(getattr(lib, creator)(self._ctx, C.byref(d), self.nrhs, fd, C.byref(h)),
-                   self._ctx)
+        if key == "NATURAL":
+            rc = getattr(lib, creator)(self._ctx, C.byref(d), self.nrhs, fd, C.byref(h))
+        else:
+            rc = getattr(lib, creator + "_ordered")(self._ctx, C.byref(d), self.nrhs, fd,
+                                                    _lib.ORDERINGS[key], C.byref(h))
+        _lib.check(rc, self._ctx)
         self._h = h
+
+    @property
+    def perm(self):
+        """perm[i] = the row of A that is row i of the factors (identity when natural)."""
+        import numpy as np
+
+        p = np.zeros(self.n, dtype=np.int32)
+        _lib.check(_lib.load().bpf_prec_permutation(self._h, p.ctypes.data_as(C.c_void_p)), self._ctx)
+        return p
 
     @property
     def handle(self):
@@ -35,12 +53,25 @@ class _DevicePrec:
 
     @property
     def P(self):
-        """The factor values on A's pattern (NVIDIA_ILU0.P / NVIDIA_IC0.P)."""
+        """The factor values on A's pattern (NVIDIA_ILU0.P / NVIDIA_IC0.P); for a reordered
+        preconditioner, on the pattern of A(perm, perm) (0-based)."""
+        import numpy as np
         import torch
 
         v = torch.empty(self.A.nnz, dtype=torch.float64, device=self.A.nzVal.device)
         _lib.check(_lib.load().bpf_prec_factor_values(self._h, v.data_ptr()), self._ctx)
-        return CuSparseMatrixCSR(self.A.rowPtr, self.A.colVal, v, self.n, self.A.index_base)
+        if self.ordering == "NATURAL":
+            return CuSparseMatrixCSR(self.A.rowPtr, self.A.colVal, v, self.n, self.A.index_base)
+        import scipy.sparse as sp
+
+        S = self.A.to_scipy()
+        perm = self.perm
+        Sh = S[perm][:, perm].tocsr()
+        Sh.sort_indices()
+        dev = self.A.nzVal.device
+        return CuSparseMatrixCSR(torch.as_tensor(Sh.indptr.astype(np.int32), device=dev),
+                                 torch.as_tensor(Sh.indices.astype(np.int32), device=dev), v,
+                                 self.n, 0)
 
     def refactor(self, vals) -> None:
         """New values on the same pattern, then the numeric factorization again."""
@@ -69,14 +100,17 @@ class NVIDIA_IC0(_DevicePrec):
     kind = "ic0"
 
 
-def ilu0(A: CuSparseMatrixCSR, nrhs: int = 1, factor_dtype: str = "float64") -> NVIDIA_ILU0:
-    """ilu0(A, nrhs) (src/preconditioners_nvidia.jl:42-47)."""
-    return NVIDIA_ILU0(A, nrhs, factor_dtype, "bpf_ilu0_create")
+def ilu0(A: CuSparseMatrixCSR, nrhs: int = 1, factor_dtype: str = "float64",
+         ordering: str = "natural") -> NVIDIA_ILU0:
+    """ilu0(A, nrhs) (src/preconditioners_nvidia.jl:42-47).  ordering="RCM" / "AMD" factors
+    A(perm, perm) instead (an addition: the reference factors A in its natural order)."""
+    return NVIDIA_ILU0(A, nrhs, factor_dtype, "bpf_ilu0_create", ordering)
 
 
-def ic0(A: CuSparseMatrixCSR, nrhs: int = 1, factor_dtype: str = "float64") -> NVIDIA_IC0:
-    """ic0(A, nrhs) (src/preconditioners_nvidia.jl:6-11)."""
-    return NVIDIA_IC0(A, nrhs, factor_dtype, "bpf_ic0_create")
+def ic0(A: CuSparseMatrixCSR, nrhs: int = 1, factor_dtype: str = "float64",
+        ordering: str = "natural") -> NVIDIA_IC0:
+    """ic0(A, nrhs) (src/preconditioners_nvidia.jl:6-11); ordering as for ilu0."""
+    return NVIDIA_IC0(A, nrhs, factor_dtype, "bpf_ic0_create", ordering)
 
 
 def ldiv_(y, P: _DevicePrec, x):

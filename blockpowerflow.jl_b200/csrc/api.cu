@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "bpf_internal.cuh"
+#include "ordering.cuh"
 #include "prec.cuh"
 
 namespace bpf {
@@ -328,20 +329,55 @@ bpf_status bpf_spmm(bpf_ctx *ctx, const bpf_csr_desc *A, int p, double alpha, co
 }
 
 static bpf_status prec_create(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs, int fdtype,
-                              int kind, bpf_prec **out) {
+                              int kind, int ordering, bpf_prec **out) {
     if (!ctx || !out) return BPF_ERR_INVALID_VALUE;
     *out = nullptr;
     if (!A) return set_error(ctx, BPF_ERR_INVALID_VALUE, "null matrix");
     if (A->dtype != BPF_F64) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "FP64 matrices only");
     if (fdtype != BPF_F64 && fdtype != BPF_F32)
         return set_error(ctx, BPF_ERR_INVALID_VALUE, "factor dtype must be BPF_F64 or BPF_F32");
+    if (ordering == BPF_ORDER_METIS)
+        return set_error(ctx, BPF_ERR_NOT_SUPPORTED,
+                         "ordering :METIS needs a METIS library, which this build does not link");
+    if (ordering < 0 || ordering > BPF_ORDER_NATURAL)
+        return set_error(ctx, BPF_ERR_INVALID_VALUE, "unknown ordering %d", ordering);
     std::vector<int> rp, ci, diag;
-    BPF_TRY(csr_pattern_to_host(ctx, A, rp, ci, true, &diag));
     int n = A->n, nnz = A->nnz;
+    std::vector<int> perm, amap;
+    if (ordering == BPF_ORDER_NATURAL) {
+        BPF_TRY(csr_pattern_to_host(ctx, A, rp, ci, true, &diag));
+    } else {
+        // A_hat = A(perm, perm): row i of A_hat is A's row perm[i], columns renumbered by the
+        // inverse permutation and sorted; amap sends A's entry k to its A_hat position.
+        std::vector<int> arp, aci;
+        BPF_TRY(csr_pattern_to_host(ctx, A, arp, aci, false, nullptr));
+        perm = ordering == BPF_ORDER_RCM ? order_rcm(n, arp, aci) : order_min_degree(n, arp, aci);
+        std::vector<int> pinv(n);
+        for (int i = 0; i < n; i++) pinv[perm[i]] = i;
+        rp.assign(n + 1, 0);
+        for (int i = 0; i < n; i++) rp[i + 1] = rp[i] + (arp[perm[i] + 1] - arp[perm[i]]);
+        ci.resize(nnz);
+        amap.resize(nnz);
+        diag.assign(n, -1);
+        std::vector<std::pair<int, int>> row;
+        for (int i = 0; i < n; i++) {
+            const int r = perm[i];
+            row.clear();
+            for (int k = arp[r]; k < arp[r + 1]; k++) row.push_back({pinv[aci[k]], k});
+            std::sort(row.begin(), row.end());
+            for (size_t t = 0; t < row.size(); t++) {
+                ci[rp[i] + t] = row[t].first;
+                amap[row[t].second] = rp[i] + (int)t;
+                if (row[t].first == i) diag[i] = rp[i] + (int)t;
+            }
+            if (diag[i] < 0) return set_error(ctx, BPF_ERR_SINGULAR, "structurally zero diagonal at row %d", r);
+        }
+    }
     bpf_prec *P = nullptr;
     BPF_TRY(prec_setup(ctx, kind, n, rp, ci, diag, &P));
     P->nrhs = nrhs;
     P->fdtype = fdtype;
+    P->ordering = ordering;
     bool ic = (kind == PREC_IC0);
     auto fail = [&](bpf_status s) {
         cudaStreamSynchronize(ctx->stream);
@@ -349,11 +385,19 @@ static bpf_status prec_create(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs, int
         return s;
     };
     bpf_status s;
-    if (nnz > 0) {
-        cudaError_t e = cudaMemcpyAsync(P->fv, A->vals, sizeof(double) * nnz, cudaMemcpyDeviceToDevice,
-                                        ctx->stream);
+    if (!perm.empty()) {
+        cudaError_t e = cudaMalloc((void **)&P->perm, sizeof(int) * n);
+        if (e == cudaSuccess && nnz > 0) e = cudaMalloc((void **)&P->amap, sizeof(int) * nnz);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(P->perm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess && nnz > 0)
+            e = cudaMemcpyAsync(P->amap, amap.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);   // host vectors die on return
         if (e != cudaSuccess) return fail(cuda_error(ctx, e, "preconditioner setup", __FILE__, __LINE__));
+        P->perm_host = perm;
+        if ((s = prec_reserve_z(ctx, P, std::max(nrhs, 1))) != BPF_SUCCESS) return fail(s);
     }
+    if ((s = prec_load_values(ctx, P, (const double *)A->vals)) != BPF_SUCCESS) return fail(s);
     if ((s = factor_numeric(ctx, P)) != BPF_SUCCESS) return fail(s);
     if ((s = tri_scatter(ctx, P->lower, P->fv)) != BPF_SUCCESS) return fail(s);
     if ((s = tri_scatter(ctx, P->upper, P->fv)) != BPF_SUCCESS) return fail(s);
@@ -364,21 +408,35 @@ static bpf_status prec_create(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs, int
 
 bpf_status bpf_ilu0_create(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs, int factor_dtype,
                            bpf_prec **prec) {
-    return prec_create(ctx, A, nrhs, factor_dtype, PREC_ILU0, prec);
+    return prec_create(ctx, A, nrhs, factor_dtype, PREC_ILU0, BPF_ORDER_NATURAL, prec);
 }
 
 bpf_status bpf_ic0_create(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs, int factor_dtype,
                           bpf_prec **prec) {
-    return prec_create(ctx, A, nrhs, factor_dtype, PREC_IC0, prec);
+    return prec_create(ctx, A, nrhs, factor_dtype, PREC_IC0, BPF_ORDER_NATURAL, prec);
+}
+
+bpf_status bpf_ilu0_create_ordered(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs, int factor_dtype,
+                                   int ordering, bpf_prec **prec) {
+    return prec_create(ctx, A, nrhs, factor_dtype, PREC_ILU0, ordering, prec);
+}
+
+bpf_status bpf_ic0_create_ordered(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs, int factor_dtype,
+                                  int ordering, bpf_prec **prec) {
+    return prec_create(ctx, A, nrhs, factor_dtype, PREC_IC0, ordering, prec);
+}
+
+bpf_status bpf_prec_permutation(const bpf_prec *P, int *perm) {
+    if (!P || (P->n > 0 && !perm)) return BPF_ERR_INVALID_VALUE;
+    for (int i = 0; i < P->n; i++) perm[i] = P->perm_host.empty() ? i : P->perm_host[i];
+    return BPF_SUCCESS;
 }
 
 bpf_status bpf_prec_refactor(bpf_prec *P, const double *vals) {
     if (!P) return BPF_ERR_INVALID_VALUE;
     bpf_ctx *ctx = P->ctx;
     if (P->nnz > 0 && !vals) return set_error(ctx, BPF_ERR_INVALID_VALUE, "null values");
-    if (P->nnz > 0)
-        BPF_CUDA(ctx, cudaMemcpyAsync(P->fv, vals, sizeof(double) * P->nnz, cudaMemcpyDeviceToDevice,
-                                      ctx->stream));
+    BPF_TRY(prec_load_values(ctx, P, vals));
     BPF_TRY(factor_numeric(ctx, P));
     BPF_TRY(tri_scatter(ctx, P->lower, P->fv));
     BPF_TRY(tri_scatter(ctx, P->upper, P->fv));
@@ -398,6 +456,7 @@ bpf_status bpf_prec_apply(bpf_prec *P, int p, const double *X, int ldx, double *
     bpf_status st;
     double *buf = (double *)ws_get(ctx, WS_A, sizeof(double) * (size_t)n * std::min(p, chunk), &st);
     if (!buf) return st;
+    BPF_TRY(prec_reserve_z(ctx, P, std::min(p, chunk)));
     for (int c0 = 0; c0 < p; c0 += chunk) {
         int pc = std::min(chunk, p - c0);
         BPF_TRY(colmajor_to_rowmajor(ctx, n, pc, X + (size_t)c0 * ldx, ldx, buf));
@@ -435,6 +494,9 @@ bpf_status bpf_prec_destroy(bpf_prec *P) {
     cudaFree(P->pdst);
     cudaFree(P->psrc);
     cudaFree(P->fv);
+    cudaFree(P->perm);
+    cudaFree(P->amap);
+    cudaFree(P->zbuf);
     delete P;
     return BPF_SUCCESS;
 }

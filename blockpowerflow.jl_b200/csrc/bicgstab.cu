@@ -241,6 +241,7 @@ extern "C" bpf_status bpf_block_bicgstab(bpf_ctx *ctx, const bpf_csr_desc *A, in
     if (n < 1 || p < 1 || !B || !X) return set_error(ctx, BPF_ERR_INVALID_VALUE, "block_bicgstab: empty system");
     if (ldb < n || ldx < n || (Cs && ldc < n)) return set_error(ctx, BPF_ERR_DIMENSION, "Inconsistent problem size");
     if (N && N->n != n) return set_error(ctx, BPF_ERR_DIMENSION, "preconditioner size differs from the system");
+    if (N) BPF_TRY(prec_reserve_z(ctx, const_cast<bpf_prec *>(N), p));
     if (p > 128) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "block_bicgstab: p=%d > 128", p);
     int itmax = opts->itmax == 0 ? 2 * n : opts->itmax;                     // :347
     const double timemax = opts->timemax > 0.0 ? opts->timemax : 1e300;

@@ -151,6 +151,9 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
                          "ILU0/IC0 preconditioners define only ldiv!: pass ldiv=true");
     if (p > n) return set_error(ctx, BPF_ERR_DIMENSION, "block_gmres: p=%d > n=%d", p, n);
     if (p > 128) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "block_gmres: p=%d > 128", p);
+    // reordered preconditioners: their scratch must hold p columns before the loop starts
+    if (M) BPF_TRY(prec_reserve_z(ctx, const_cast<bpf_prec *>(M), p));
+    if (N) BPF_TRY(prec_reserve_z(ctx, const_cast<bpf_prec *>(N), p));
     int memory = std::min(n / p, opts->memory);
     if (memory < 1) memory = 1;
     const bool restart = opts->restart != 0;

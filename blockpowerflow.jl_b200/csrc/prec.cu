@@ -377,7 +377,7 @@ bpf_status factor_numeric(bpf_ctx *ctx, bpf_prec *P) {
 template <int G, int CPL, typename TF, bool IN_F32, bool OUT_F32>
 __global__ void __launch_bounds__(512)
 trsv2_coop_kernel(TriKernelArgs t0, TriKernelArgs t1, int p, const void *Xv, void *Yv,
-                  DevStatus *ds, const int *gate) {
+                  DevStatus *ds, const int *gate, const int *perm, double *Zv) {
     if (gate && *gate == 0) return;
     __shared__ unsigned s_gen;
     if (threadIdx.x == 0) s_gen = barrier_gen_start(ds);
@@ -386,7 +386,11 @@ trsv2_coop_kernel(TriKernelArgs t0, TriKernelArgs t1, int p, const void *Xv, voi
     using TIn = typename std::conditional<IN_F32, float, double>::type;
     using TOut = typename std::conditional<OUT_F32, float, double>::type;
     const TIn *X = (const TIn *)Xv;
-    TOut *Y = (TOut *)Yv;
+    TOut *Yout = (TOut *)Yv;
+    // Reordered factors (perm != null): the forward sweep gathers X's rows through perm and
+    // writes the factor-ordered Z; the backward sweep reads Z and scatters Y's rows through
+    // perm.  Otherwise both sweeps work in place in Y.
+    TOut *Zf = perm ? (TOut *)Zv : Yout;
     const int lane = threadIdx.x & 31;
     const int glane = lane % G;
     const int gpb = blockDim.x / G;
@@ -402,13 +406,15 @@ trsv2_coop_kernel(TriKernelArgs t0, TriKernelArgs t1, int p, const void *Xv, voi
             const int q0 = __ldg(t.lev_ptr + l), q1 = __ldg(t.lev_ptr + l + 1);
             for (int q = q0 + gid; q < q1; q += ng) {
                 const int i = __ldg(t.rows + q);
+                const int io = perm ? __ldg(perm + i) : i;   // row of i in the caller's order
+                TOut *Y = (phase == 0) ? Zf : Yout;          // the sweep's solved rows
                 TF acc[CPL];
 #pragma unroll
                 for (int j = 0; j < CPL; j++) {
                     const int col = glane + j * G;
                     if (col < p) {
-                        if (phase == 0) acc[j] = (TF)X[(size_t)i * p + col];
-                        else acc[j] = (TF)__ldcg(Y + (size_t)i * p + col);
+                        if (phase == 0) acc[j] = (TF)X[(size_t)io * p + col];
+                        else acc[j] = (TF)__ldcg(Zf + (size_t)i * p + col);
                     } else {
                         acc[j] = (TF)0;
                     }
@@ -423,8 +429,10 @@ trsv2_coop_kernel(TriKernelArgs t0, TriKernelArgs t1, int p, const void *Xv, voi
                         a = __ldg(val + k);
                     }
                     const int cnt = min(G, re - kb);
+                    int co = 0;
+                    if (k < re && perm && phase == 1) co = __ldg(perm + c);
                     for (int s = 0; s < cnt; s++) {
-                        const int cs = __shfl_sync(gmask, c, s, G);
+                        const int cs = __shfl_sync(gmask, (perm && phase == 1) ? co : c, s, G);
                         const TF as = __shfl_sync(gmask, a, s, G);
                         const TOut *yr = Y + (size_t)cs * p;
 #pragma unroll
@@ -436,7 +444,7 @@ trsv2_coop_kernel(TriKernelArgs t0, TriKernelArgs t1, int p, const void *Xv, voi
                 }
                 TF dv = (TF)1;
                 if (dinv) dv = __ldg(dinv + q);
-                TOut *yi = Y + (size_t)i * p;
+                TOut *yi = Y + (size_t)((phase == 1) ? io : i) * p;
 #pragma unroll
                 for (int j = 0; j < CPL; j++) {
                     const int col = glane + j * G;
@@ -453,7 +461,8 @@ trsv2_coop_kernel(TriKernelArgs t0, TriKernelArgs t1, int p, const void *Xv, voi
 
 template <int G, int CPL, typename TF, bool IN_F32, bool OUT_F32>
 static bpf_status launch_trsv2(bpf_ctx *ctx, const TriDev &t0, const TriDev &t1, int p,
-                               const void *X, void *Y, const int *gate) {
+                               const void *X, void *Y, const int *gate, const int *perm,
+                               double *Z) {
     auto kern = trsv2_coop_kernel<G, CPL, TF, IN_F32, OUT_F32>;
     const int maxrows = std::max(t0.max_level_rows, t1.max_level_rows);
     int threads, grid;
@@ -471,7 +480,7 @@ static bpf_status launch_trsv2(bpf_ctx *ctx, const TriDev &t0, const TriDev &t1,
     }
     TriKernelArgs a0 = t0.args(), a1 = t1.args();
     DevStatus *ds = ctx->dstat;
-    void *args[] = {&a0, &a1, &p, (void *)&X, &Y, &ds, (void *)&gate};
+    void *args[] = {&a0, &a1, &p, (void *)&X, &Y, &ds, (void *)&gate, (void *)&perm, &Z};
     // Algorithmic bytes: (4 + sizeof(TF)) per off-diagonal entry of both factors, the
     // diagonal inverses, row pointers and row ids, and 4 n p vector values (read X, write Y,
     // read and write Y in the backward sweep).
@@ -488,14 +497,15 @@ static bpf_status launch_trsv2(bpf_ctx *ctx, const TriDev &t0, const TriDev &t1,
 
 template <typename TF, bool IN_F32, bool OUT_F32>
 static bpf_status trsv2_dispatch(bpf_ctx *ctx, const TriDev &t0, const TriDev &t1, int p,
-                                 const void *X, void *Y, const int *gate) {
-    if (p <= 4) return launch_trsv2<4, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
-    if (p <= 8) return launch_trsv2<8, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
-    if (p <= 16) return launch_trsv2<16, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
-    if (p <= 32) return launch_trsv2<32, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
-    if (p <= 64) return launch_trsv2<32, 2, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
-    if (p <= 128) return launch_trsv2<32, 4, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
-    if (p <= 256) return launch_trsv2<32, 8, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate);
+                                 const void *X, void *Y, const int *gate, const int *perm,
+                                 double *Z) {
+    if (p <= 4) return launch_trsv2<4, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate, perm, Z);
+    if (p <= 8) return launch_trsv2<8, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate, perm, Z);
+    if (p <= 16) return launch_trsv2<16, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate, perm, Z);
+    if (p <= 32) return launch_trsv2<32, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate, perm, Z);
+    if (p <= 64) return launch_trsv2<32, 2, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate, perm, Z);
+    if (p <= 128) return launch_trsv2<32, 4, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate, perm, Z);
+    if (p <= 256) return launch_trsv2<32, 8, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate, perm, Z);
     return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "triangular solve: p=%d > 256 per call", p);
 }
 
@@ -504,9 +514,44 @@ static bpf_status trsv2_dispatch(bpf_ctx *ctx, const TriDev &t0, const TriDev &t
 bpf_status prec_apply_rowmajor(bpf_ctx *ctx, const bpf_prec *P, int p, const double *X,
                                double *Y, const int *gate) {
     if (P->n == 0 || p == 0) return BPF_SUCCESS;
+    if (P->perm && p > P->zcols)
+        return set_error(ctx, BPF_ERR_NOT_SUPPORTED,
+                         "reordered preconditioner: %d right-hand sides exceed the %d-column scratch "
+                         "reserved for it", p, P->zcols);
     if (P->fdtype == BPF_F32)
-        return trsv2_dispatch<float, false, false>(ctx, P->lower, P->upper, p, X, Y, gate);
-    return trsv2_dispatch<double, false, false>(ctx, P->lower, P->upper, p, X, Y, gate);
+        return trsv2_dispatch<float, false, false>(ctx, P->lower, P->upper, p, X, Y, gate, P->perm, P->zbuf);
+    return trsv2_dispatch<double, false, false>(ctx, P->lower, P->upper, p, X, Y, gate, P->perm, P->zbuf);
+}
+
+bpf_status prec_reserve_z(bpf_ctx *ctx, bpf_prec *P, int p) {
+    if (!P->perm || p <= P->zcols) return BPF_SUCCESS;
+    const int cols = std::min(std::max(p, 1), 256);
+    double *z = nullptr;
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    BPF_CUDA(ctx, cudaMalloc((void **)&z, sizeof(double) * (size_t)P->n * cols));
+    if (P->zbuf) cudaFree(P->zbuf);
+    P->zbuf = z;
+    P->zcols = cols;
+    return BPF_SUCCESS;
+}
+
+__global__ void scatter_map_kernel(int nnz, const double *__restrict__ vals, const int *__restrict__ map,
+                                   double *__restrict__ out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += gridDim.x * blockDim.x)
+        out[__ldg(map + k)] = vals[k];
+}
+
+bpf_status prec_load_values(bpf_ctx *ctx, bpf_prec *P, const double *vals) {
+    if (P->nnz == 0) return BPF_SUCCESS;
+    if (!P->amap) {
+        BPF_CUDA(ctx, cudaMemcpyAsync(P->fv, vals, sizeof(double) * P->nnz, cudaMemcpyDeviceToDevice,
+                                      ctx->stream));
+        return BPF_SUCCESS;
+    }
+    const int blocks = std::max(1, std::min(ceil_div(P->nnz, 256), ctx->num_sms * 8));
+    scatter_map_kernel<<<blocks, 256, 0, ctx->stream>>>(P->nnz, vals, P->amap, P->fv);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
 }
 
 }  // namespace bpf

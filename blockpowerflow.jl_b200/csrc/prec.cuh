@@ -85,6 +85,14 @@ struct bpf_prec {
     long long npairs = 0;
     bpf::TriDev lower;   // forward solve (L unit for ILU0; L for IC0)
     bpf::TriDev upper;   // backward solve (U for ILU0; L' for IC0)
+    // Symmetric reordering (bpf_ilu0_create_ordered): the factors are those of A_hat =
+    // A(perm, perm); perm[i] = original row of factor row i; amap[k] = position of A's entry
+    // k in A_hat's pattern; zbuf = n x zcols factor-ordered scratch of the solves.
+    int ordering = BPF_ORDER_NATURAL;
+    int *perm = nullptr, *amap = nullptr;
+    std::vector<int> perm_host;
+    double *zbuf = nullptr;
+    int zcols = 0;
 };
 
 namespace bpf {
@@ -95,4 +103,9 @@ bpf_status csr_pattern_to_host(bpf_ctx *ctx, const bpf_csr_desc *A, std::vector<
 bpf_status factor_numeric(bpf_ctx *ctx, bpf_prec *P);
 bpf_status prec_apply_rowmajor(bpf_ctx *ctx, const bpf_prec *P, int p, const double *X,
                                double *Y, const int *gate = nullptr);
+// Reordered preconditioners: make the factor-ordered scratch hold p columns (allocates when it
+// grows; prec_apply_rowmajor itself never allocates and rejects p > zcols).
+bpf_status prec_reserve_z(bpf_ctx *ctx, bpf_prec *P, int p);
+// A's values into the factor storage (a copy, or the scatter through amap when reordered).
+bpf_status prec_load_values(bpf_ctx *ctx, bpf_prec *P, const double *vals);
 }  // namespace bpf

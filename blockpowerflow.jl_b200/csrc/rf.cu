@@ -23,121 +23,10 @@
 #include <vector>
 
 #include "bpf_internal.cuh"
+#include "ordering.cuh"
 #include "prec.cuh"
 
 namespace bpf {
-
-// ------------------------------------------------------------------------------------
-// orderings
-// ------------------------------------------------------------------------------------
-static void sym_adjacency(int n, const std::vector<int> &rp, const std::vector<int> &ci,
-                          std::vector<std::vector<int>> &adj) {
-    adj.assign(n, {});
-    for (int i = 0; i < n; i++)
-        for (int k = rp[i]; k < rp[i + 1]; k++) {
-            int j = ci[k];
-            if (j == i) continue;
-            adj[i].push_back(j);
-            adj[j].push_back(i);
-        }
-    for (auto &a : adj) {
-        std::sort(a.begin(), a.end());
-        a.erase(std::unique(a.begin(), a.end()), a.end());
-    }
-}
-
-// Minimum degree on the explicit elimination graph: eliminate a node of least current
-// degree (smallest index on ties), turning its neighbourhood into a clique.
-static std::vector<int> order_min_degree(int n, const std::vector<int> &rp, const std::vector<int> &ci) {
-    std::vector<std::vector<int>> adj;
-    sym_adjacency(n, rp, ci, adj);
-    std::set<std::pair<int, int>> pq;
-    std::vector<int> deg(n);
-    for (int v = 0; v < n; v++) {
-        deg[v] = (int)adj[v].size();
-        pq.insert({deg[v], v});
-    }
-    std::vector<int> order;
-    order.reserve(n);
-    std::vector<int> merged;
-    while (!pq.empty()) {
-        const int v = pq.begin()->second;
-        pq.erase(pq.begin());
-        order.push_back(v);
-        const std::vector<int> nb = adj[v];
-        for (int u : nb) {
-            merged.clear();
-            std::set_union(adj[u].begin(), adj[u].end(), nb.begin(), nb.end(), std::back_inserter(merged));
-            merged.erase(std::remove_if(merged.begin(), merged.end(), [&](int w) { return w == u || w == v; }),
-                         merged.end());
-            pq.erase({deg[u], u});
-            adj[u].swap(merged);
-            deg[u] = (int)adj[u].size();
-            pq.insert({deg[u], u});
-        }
-        adj[v].clear();
-        adj[v].shrink_to_fit();
-    }
-    return order;
-}
-
-static std::vector<int> bfs_levels(int s, const std::vector<std::vector<int>> &adj,
-                                   std::vector<int> &lev, const std::vector<char> &done) {
-    std::vector<int> q{s};
-    lev.assign(adj.size(), -1);
-    lev[s] = 0;
-    for (size_t h = 0; h < q.size(); h++) {
-        int v = q[h];
-        for (int u : adj[v])
-            if (lev[u] < 0 && !done[u]) {
-                lev[u] = lev[v] + 1;
-                q.push_back(u);
-            }
-    }
-    return q;
-}
-
-// Reverse Cuthill-McKee from a pseudo-peripheral start node of each component.
-static std::vector<int> order_rcm(int n, const std::vector<int> &rp, const std::vector<int> &ci) {
-    std::vector<std::vector<int>> adj;
-    sym_adjacency(n, rp, ci, adj);
-    std::vector<char> done(n, 0);
-    std::vector<int> order, lev;
-    order.reserve(n);
-    for (int seed = 0; seed < n; seed++) {
-        if (done[seed]) continue;
-        // pseudo-peripheral node (George-Liu)
-        int s = seed, ecc = -1;
-        for (int it = 0; it < 8; it++) {
-            std::vector<int> comp = bfs_levels(s, adj, lev, done);
-            int e = lev[comp.back()];
-            if (e <= ecc) break;
-            ecc = e;
-            int best = comp.back();
-            for (int v : comp)
-                if (lev[v] == e && adj[v].size() < adj[best].size()) best = v;
-            s = best;
-        }
-        std::vector<int> q{s};
-        done[s] = 1;
-        for (size_t h = 0; h < q.size(); h++) {
-            int v = q[h];
-            std::vector<int> nb;
-            for (int u : adj[v])
-                if (!done[u]) nb.push_back(u);
-            std::sort(nb.begin(), nb.end(), [&](int a, int b) {
-                return adj[a].size() < adj[b].size() || (adj[a].size() == adj[b].size() && a < b);
-            });
-            for (int u : nb) {
-                done[u] = 1;
-                q.push_back(u);
-            }
-        }
-        order.insert(order.end(), q.begin(), q.end());
-    }
-    std::reverse(order.begin(), order.end());
-    return order;
-}
 
 // ------------------------------------------------------------------------------------
 // left-looking sparse LU with threshold partial pivoting (Gilbert-Peierls)

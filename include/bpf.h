@@ -169,6 +169,22 @@ BPF_API bpf_status bpf_ilu0_create(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs
 /* ic0(A, nrhs) -- src/preconditioners_nvidia.jl:6-11 (csric02 on A's lower triangle). */
 BPF_API bpf_status bpf_ic0_create(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs,
                                   int factor_dtype, bpf_prec **prec);
+
+/* ilu0 / ic0 with a symmetric reordering of the pattern: the factors are those of
+ * A(perm, perm), and bpf_prec_apply keeps ldiv! semantics in A's own ordering (y = M \ x with
+ * M = P' L U P).  No counterpart in the reference, whose ilu0 / ic0 factor A in its natural
+ * order (src/preconditioners_nvidia.jl:6-11,42-47); the orderings are those of the RF analysis
+ * (src/cusolverRF.jl:70-95): BPF_ORDER_RCM (reverse Cuthill-McKee), BPF_ORDER_AMD / MDQ
+ * (minimum degree), BPF_ORDER_NATURAL (same as bpf_ilu0_create); BPF_ORDER_METIS is not
+ * available.  nrhs sizes the factor-ordered scratch of the solves (grown on demand by
+ * bpf_prec_apply and the Krylov solvers; bpf_prec_apply_noalloc uses it as it is). */
+BPF_API bpf_status bpf_ilu0_create_ordered(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs,
+                                           int factor_dtype, int ordering, bpf_prec **prec);
+BPF_API bpf_status bpf_ic0_create_ordered(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs,
+                                          int factor_dtype, int ordering, bpf_prec **prec);
+/* The preconditioner's ordering: perm[i] = the row of A that is row i of the factors (the
+ * identity for a natural-order preconditioner); perm is a host array of n ints. */
+BPF_API bpf_status bpf_prec_permutation(const bpf_prec *P, int *perm);
 /* New values on the same pattern (device pointer, nnz doubles), then refactor.  The
  * reference rebuilds the preconditioner with ilu0(A) after each Jacobian update
  * (benchmarks/benchmarks_nvidia.jl:44). */
