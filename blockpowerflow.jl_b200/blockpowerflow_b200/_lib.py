@@ -87,6 +87,7 @@ SIGNATURES = {
     "bpf_ilu0_create_ordered": (_I, [_P, C.POINTER(CsrDesc), _I, _I, _I, C.POINTER(_P)]),
     "bpf_ic0_create_ordered": (_I, [_P, C.POINTER(CsrDesc), _I, _I, _I, C.POINTER(_P)]),
     "bpf_prec_permutation": (_I, [_P, _P]),
+    "bpf_tc_gemm_bf16": (_I, [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I]),
     "bpf_prec_refactor": (_I, [_P, _P]),
     "bpf_prec_apply": (_I, [_P, _I, _P, _I, _P, _I]),
     "bpf_prec_apply_noalloc": (_I, [_P, _I, _P, _I, _P, _I]),
@@ -180,7 +181,7 @@ def kernel_launches(device=None) -> int:
 
 
 KERNEL_CLASSES = {"spmm": 0, "trsv": 1, "factor": 2, "gram": 3, "tsmm": 4, "small": 5,
-                  "chol": 6, "hess": 7, "backsub": 8}
+                  "chol": 6, "hess": 7, "backsub": 8, "mlp": 9}
 
 
 def set_timing(on: bool, device=None) -> None:

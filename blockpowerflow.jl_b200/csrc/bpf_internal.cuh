@@ -56,6 +56,7 @@ enum Slot : int {
     WS_VEC,           // n x p working blocks of a solve
     WS_Y,             // block back-substitution result Y
     WS_ZB,            // flexible GMRES: preconditioned basis blocks
+    WS_FLAGS,         // small device status words (tensor-core GEMM errors)
     WS_COUNT
 };
 

@@ -113,23 +113,31 @@ mutable struct NVIDIA_IC0
 end
 const DevicePrec = Union{NVIDIA_ILU0,NVIDIA_IC0}
 
-function _prec(fn::Symbol, A, nrhs, factor_type)
+const PREC_ORDER = Dict(:natural => 4, :AMD => 0, :MDQ => 1, :METIS => 2, :RCM => 3)
+
+function _prec(fn::Symbol, A, nrhs, factor_type, ordering)
     r = Ref{Ptr{Cvoid}}(C_NULL)
     d = Ref(desc(A))
     fd = factor_type === Float32 ? 1 : 0
-    check(ccall((fn, libbpf), Cint, (Ptr{Cvoid}, Ref{CsrDesc}, Cint, Cint, Ref{Ptr{Cvoid}}),
-                ctx(), d, nrhs, fd, r))
+    if ordering === :natural
+        check(ccall((fn, libbpf), Cint, (Ptr{Cvoid}, Ref{CsrDesc}, Cint, Cint, Ref{Ptr{Cvoid}}),
+                    ctx(), d, nrhs, fd, r))
+    else   # an addition: the reference factors A in its natural order
+        check(ccall((Symbol(fn, :_ordered), libbpf), Cint,
+                    (Ptr{Cvoid}, Ref{CsrDesc}, Cint, Cint, Cint, Ref{Ptr{Cvoid}}),
+                    ctx(), d, nrhs, fd, PREC_ORDER[ordering], r))
+    end
     return r[]
 end
 
-function ilu0(A::CuSparseMatrixCSR{Float64,Cint}, nrhs::Int; factor_type=Float64)
-    P = NVIDIA_ILU0(_prec(:bpf_ilu0_create, A, nrhs, factor_type), size(A, 1))
+function ilu0(A::CuSparseMatrixCSR{Float64,Cint}, nrhs::Int; factor_type=Float64, ordering=:natural)
+    P = NVIDIA_ILU0(_prec(:bpf_ilu0_create, A, nrhs, factor_type, ordering), size(A, 1))
     finalizer(p -> ccall((:bpf_prec_destroy, libbpf), Cint, (Ptr{Cvoid},), p.h), P)
     return P
 end
 
-function ic0(A::CuSparseMatrixCSR{Float64,Cint}, nrhs::Int; factor_type=Float64)
-    P = NVIDIA_IC0(_prec(:bpf_ic0_create, A, nrhs, factor_type), size(A, 1))
+function ic0(A::CuSparseMatrixCSR{Float64,Cint}, nrhs::Int; factor_type=Float64, ordering=:natural)
+    P = NVIDIA_IC0(_prec(:bpf_ic0_create, A, nrhs, factor_type, ordering), size(A, 1))
     finalizer(p -> ccall((:bpf_prec_destroy, libbpf), Cint, (Ptr{Cvoid},), p.h), P)
     return P
 end

@@ -141,7 +141,8 @@ typedef enum {
     BPF_KC_CHOL = 6,    /* Cholesky-QR: Cholesky + inverse of p x p Gram */
     BPF_KC_HESS = 7,    /* block Hessenberg QR update (apply + factor) */
     BPF_KC_BACKSUB = 8, /* block back substitution of block-GMRES     */
-    BPF_KC_COUNT = 9
+    BPF_KC_MLP = 9,     /* learned warm start: tensor-core GEMMs       */
+    BPF_KC_COUNT = 10
 } bpf_kernel_class;
 BPF_API bpf_status bpf_ctx_set_timing(bpf_ctx *ctx, int on);
 /* Totals since bpf_ctx_set_timing(ctx, 1): device milliseconds, launches, and the launches'
@@ -149,6 +150,15 @@ BPF_API bpf_status bpf_ctx_set_timing(bpf_ctx *ctx, int on);
  * beside it in the sources).  Any output pointer may be NULL. */
 BPF_API bpf_status bpf_ctx_kernel_time(bpf_ctx *ctx, int kernel_class, double *total_ms,
                                        long long *launches, double *bytes, double *flops);
+
+/* ---- tensor-core GEMM of the learned warm start ------------------------------------------
+ * D (M x N, FP32, row stride ldd) = [D +] A (M x K) B (N x K)^T with A and B row-major BF16
+ * (K contiguous; lda, ldb multiples of 8; K a multiple of 64), on the tcgen05 tensor cores
+ * with the accumulator in TMEM; splits = K slices (0: chosen to fill the GPU).  No counterpart
+ * in the reference (whose solvers have no learned part); the building block of bpf_mlp_*. */
+BPF_API bpf_status bpf_tc_gemm_bf16(bpf_ctx *ctx, int M, int N, int K, const void *A, int lda,
+                                    const void *B, int ldb, float *D, int ldd, int accumulate,
+                                    int splits);
 
 /* ---- sparse x dense block -------------------------------------------------------------- */
 /* Y = alpha*A*X + beta*Y: mul!(W, A, P) of src/block_gmres.jl:299 (CSR SpMM). */
