@@ -88,6 +88,17 @@ SIGNATURES = {
     "bpf_ic0_create_ordered": (_I, [_P, C.POINTER(CsrDesc), _I, _I, _I, C.POINTER(_P)]),
     "bpf_prec_permutation": (_I, [_P, _P]),
     "bpf_tc_gemm_bf16": (_I, [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I]),
+    "bpf_mlp_create": (_I, [_P, _I, _I, C.c_ulonglong, C.POINTER(_P)]),
+    "bpf_mlp_destroy": (_I, [_P]),
+    "bpf_mlp_set_scale": (_I, [_P, _D]),
+    "bpf_mlp_forward": (_I, [_P, _I, _P, _I, _P, _I]),
+    "bpf_mlp_gradients": (_I, [_P, _I, _P, _I, _P, _I, C.POINTER(_D)]),
+    "bpf_mlp_train_step": (_I, [_P, _I, _P, _I, _P, _I, _D, C.POINTER(_D)]),
+    "bpf_mlp_params": (_I, [_P, _I, C.POINTER(_P), C.POINTER(_P), C.POINTER(C.c_longlong),
+                            C.POINTER(C.c_longlong)]),
+    "bpf_mlp_refresh": (_I, [_P]),
+    "bpf_mlp_param_copy": (_I, [_P, _I, _I, _P, _I]),
+    "bpf_mlp_basis": (_I, [_P, _I, C.c_ulonglong, _P, _I]),
     "bpf_prec_refactor": (_I, [_P, _P]),
     "bpf_prec_apply": (_I, [_P, _I, _P, _I, _P, _I]),
     "bpf_prec_apply_noalloc": (_I, [_P, _I, _P, _I, _P, _I]),
@@ -96,6 +107,8 @@ SIGNATURES = {
     "bpf_prec_destroy": (_I, [_P]),
     "bpf_block_gmres": (_I, [_P, C.POINTER(CsrDesc), _I, _P, _I, _P, _I, _P, _I, _P, _P,
                              C.POINTER(GmresOpts), C.POINTER(Stats)]),
+    "bpf_block_gmres_deflated": (_I, [_P, C.POINTER(CsrDesc), _I, _P, _I, _P, _I, _P, _I, _P, _P,
+                             C.POINTER(GmresOpts), _P, _I, _I, C.POINTER(Stats)]),
     "bpf_block_bicgstab": (_I, [_P, C.POINTER(CsrDesc), _I, _P, _I, _P, _I, _P, _I, _P,
                                 C.POINTER(BicgstabOpts), C.POINTER(Stats)]),
     "bpf_rf_analyze": (_I, [_P, C.POINTER(CsrDesc), _I, _D, _I, _I, C.POINTER(_P)]),

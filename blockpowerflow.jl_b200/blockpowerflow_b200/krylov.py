@@ -51,10 +51,13 @@ def _prec_handle(P):
 def block_gmres(A: CuSparseMatrixCSR, B, X0=None, *, memory: int = 20, M=None, N=None,
                 ldiv: bool = False, restart: bool = False, reorthogonalization: bool = False,
                 atol: float = _SQRT_EPS, rtol: float = _SQRT_EPS, itmax: int = 0,
-                timemax: float = math.inf, verbose: int = 0, history: bool = False):
+                timemax: float = math.inf, verbose: int = 0, history: bool = False,
+                deflation=None):
     """(X, stats) = block_gmres(A, B[, X0]; kwargs...)  (src/block_gmres.jl:127-154).
 
     M / N: left / right preconditioner (None = identity), applied with ldiv! when ldiv=True.
+    deflation: an n x r basis (r <= p) to augment the Krylov space with (GCRO form); an
+    addition of this build, typically the learned basis of learned.WarmStartMLP.basis.
     """
     Bc = colmajor(B)
     n, p = Bc.shape
@@ -77,9 +80,18 @@ def block_gmres(A: CuSparseMatrixCSR, B, X0=None, *, memory: int = 20, M=None, N
     res = np.zeros(max(cap, 1))
     st = _lib.Stats(0, 0, 0, 0.0, 0, len(res), res.ctypes.data_as(C.POINTER(C.c_double)), 0)
     d = A.desc()
-    _lib.check(lib.bpf_block_gmres(ctx, C.byref(d), p, Bc.data_ptr(), ld(Bc), X.data_ptr(), ld(X),
-                                   x0p, ldx0, _prec_handle(M), _prec_handle(N), C.byref(opts),
-                                   C.byref(st)), ctx)
+    if deflation is None:
+        _lib.check(lib.bpf_block_gmres(ctx, C.byref(d), p, Bc.data_ptr(), ld(Bc), X.data_ptr(), ld(X),
+                                       x0p, ldx0, _prec_handle(M), _prec_handle(N), C.byref(opts),
+                                       C.byref(st)), ctx)
+    else:
+        Zc = colmajor(deflation)
+        if Zc.shape[0] != n:
+            raise _lib.DimensionMismatch(_lib.BPF_ERR_DIMENSION, "deflation basis must have n rows")
+        _lib.check(lib.bpf_block_gmres_deflated(ctx, C.byref(d), p, Bc.data_ptr(), ld(Bc), X.data_ptr(),
+                                                ld(X), x0p, ldx0, _prec_handle(M), _prec_handle(N),
+                                                C.byref(opts), Zc.data_ptr(), ld(Zc), Zc.shape[1],
+                                                C.byref(st)), ctx)
     stats = BlockGMRESStats(st.niter, bool(st.solved),
                             res[: min(st.n_residuals, len(res))].tolist() if history else [],
                             st.timer, _status_string(st.status), st.npass)

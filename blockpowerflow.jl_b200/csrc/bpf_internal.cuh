@@ -57,6 +57,7 @@ enum Slot : int {
     WS_Y,             // block back-substitution result Y
     WS_ZB,            // flexible GMRES: preconditioned basis blocks
     WS_FLAGS,         // small device status words (tensor-core GEMM errors)
+    WS_DEFL,          // deflated block-GMRES: Q_C, Z R^{-1}, E_j blocks
     WS_COUNT
 };
 

@@ -98,6 +98,31 @@ static double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// dst (n x p, row-major) = src (n x r, row-major) in the first r columns, zeros after.
+__global__ void pad_cols_kernel(int n, int r, int p, const double *__restrict__ src, double *__restrict__ dst) {
+    const size_t total = (size_t)n * p;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = e / p;
+        const int c = (int)(e % p);
+        dst[e] = c < r ? src[i * r + c] : 0.0;
+    }
+}
+
+// Columns c0 <= c < c1 of the row-major n x p block X set to zero.
+__global__ void zero_cols_kernel(int n, int c0, int c1, int p, double *__restrict__ X) {
+    const size_t total = (size_t)n * (c1 - c0);
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x)
+        X[(e / (c1 - c0)) * p + c0 + e % (c1 - c0)] = 0.0;
+}
+
+// Deflation state of one solve (GCRO form): Q_C = A Z R^{-1} orthonormal (n x r, zero-padded
+// to p columns), Zd = Z R^{-1} (so that A Zd = Q_C), E_j = Q_C^T (A N^{-1} V_j) per iteration
+// and the accumulated correction Xdef of the current pass.
+struct Deflation {
+    int r = 0;
+    double *Qp = nullptr, *Zp = nullptr, *Xdef = nullptr, *E = nullptr, *E2 = nullptr, *F = nullptr;
+};
+
 struct GmresBufs {
     double *V, *Rblk, *HY, *tau, *Z;
     double *Zb;   // flexible form: preconditioned basis N \ V_i (null otherwise)
@@ -131,11 +156,10 @@ static bpf_status gmres_capacity(bpf_ctx *ctx, int n, int p, int cap, int old_ca
 
 using namespace bpf;
 
-extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p,
-                                      const double *B, int ldb, double *X, int ldx,
-                                      const double *X0, int ldx0, const bpf_prec *M,
-                                      const bpf_prec *N, const bpf_gmres_opts *opts,
-                                      bpf_stats *stats) {
+static bpf_status block_gmres_impl(bpf_ctx *ctx, const bpf_csr_desc *A, int p, const double *B,
+                                   int ldb, double *X, int ldx, const double *X0, int ldx0,
+                                   const bpf_prec *M, const bpf_prec *N, const bpf_gmres_opts *opts,
+                                   bpf_stats *stats, const double *Zdef, int ldz, int rdef) {
     if (!ctx) return BPF_ERR_INVALID_VALUE;
     const double t0 = now_s();
     if (!A || !opts || !stats) return set_error(ctx, BPF_ERR_INVALID_VALUE, "block_gmres: null argument");
@@ -151,6 +175,12 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
                          "ILU0/IC0 preconditioners define only ldiv!: pass ldiv=true");
     if (p > n) return set_error(ctx, BPF_ERR_DIMENSION, "block_gmres: p=%d > n=%d", p, n);
     if (p > 128) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "block_gmres: p=%d > 128", p);
+    if (rdef > 0) {
+        if (!Zdef || ldz < n) return set_error(ctx, BPF_ERR_INVALID_VALUE, "block_gmres: deflation basis");
+        if (rdef > p)
+            return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "block_gmres: deflation rank %d > p = %d", rdef, p);
+        if (M) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "block_gmres: deflation with a left preconditioner");
+    }
     // reordered preconditioners: their scratch must hold p columns before the loop starts
     if (M) BPF_TRY(prec_reserve_z(ctx, const_cast<bpf_prec *>(M), p));
     if (N) BPF_TRY(prec_reserve_z(ctx, const_cast<bpf_prec *>(N), p));
@@ -209,6 +239,7 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
     SolveState hs;
     std::memset(&hs, 0, sizeof(hs));
     hs.itmax = itmax;
+    hs.active = 1;   // lets the set-up products run; gmres_init_kernel decides the first pass
     hs.qr_fail_iter = 0x7fffffff;
     hs.inner_itmax = itmax;
     hs.mem = memory;
@@ -234,6 +265,65 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
     }
     if (M) BPF_TRY(prec_apply_rowmajor(ctx, M, p, W, Qm));
     BPF_TRY(frob_norm(ctx, np, R0, &st->rnorm));
+    Deflation dfl;
+    if (rdef > 0) {
+        // Q_C = A Z R^{-1} by Cholesky-QR (R on the host for its inverse), Zd = Z R^{-1}
+        const int r = rdef;
+        const size_t nr = (size_t)n * r;
+        double *dw = (double *)ws_get(ctx, WS_DEFL, sizeof(double) * (4 * nr + 3 * np + (size_t)(itmax + 2) * pp +
+                                                                      2 * pp + 2 * (size_t)r * r), &s);
+        if (!dw) return s;
+        double *Zc = dw, *Cc = dw + nr, *Qc = dw + 2 * nr, *Tc = dw + 3 * nr;
+        dfl.r = r;
+        dfl.Qp = dw + 4 * nr;
+        dfl.Zp = dfl.Qp + np;
+        dfl.Xdef = dfl.Zp + np;
+        dfl.E = dfl.Xdef + np;
+        dfl.E2 = dfl.E + (size_t)(itmax + 2) * pp;
+        dfl.F = dfl.E2 + pp;
+        double *Rr = dfl.F + pp, *Rinv = Rr + (size_t)r * r;
+        BPF_TRY(colmajor_to_rowmajor(ctx, n, r, Zdef, ldz, Zc));
+        BPF_TRY(spmm_rowmajor(ctx, n, A->nnz, rp, ci, av, base, r, 1.0, Zc, 0.0, Cc, nullptr));
+        BPF_TRY(cholqr(ctx, n, r, Cc, Qc, Rr, Tc, st));
+        std::vector<double> Rh((size_t)r * r), Ri((size_t)r * r, 0.0);
+        BPF_CUDA(ctx, cudaMemcpyAsync(Rh.data(), Rr, sizeof(double) * Rh.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        BPF_TRY(check_dev_status(ctx, "block_gmres deflation basis"));
+        // Keep the leading columns whose pivots are well conditioned: a (numerically) dependent
+        // column would make Z R^{-1} blow up and break A Zd = Q_C, on which the residual
+        // estimate rests.  A basis with no usable column deflates nothing.
+        double rmax = 0.0;
+        for (int c = 0; c < r; c++) rmax = std::max(rmax, std::fabs(Rh[(size_t)c * r + c]));
+        int r_ok = 0;
+        while (r_ok < r && std::isfinite(Rh[(size_t)r_ok * r + r_ok]) &&
+               std::fabs(Rh[(size_t)r_ok * r + r_ok]) > 1e-8 * rmax)
+            r_ok++;
+        for (int c = 0; c < r; c++) {   // upper-triangular inverse, column by column
+            for (int i = c; i >= 0; i--) {
+                double v = (i == c) ? 1.0 : 0.0;
+                for (int k = i + 1; k <= c; k++) v -= Rh[(size_t)i * r + k] * Ri[(size_t)k * r + c];
+                Ri[(size_t)i * r + c] = v / Rh[(size_t)i * r + i];
+            }
+        }
+        // columns >= r_ok of Q_C and Zd are zeroed (their R^{-1} columns are dropped)
+        for (int c = r_ok; c < r; c++)
+            for (int i = 0; i < r; i++) Ri[(size_t)i * r + c] = 0.0;
+        BPF_CUDA(ctx, cudaMemcpyAsync(Rinv, Ri.data(), sizeof(double) * Ri.size(), cudaMemcpyHostToDevice, ctx->stream));
+        BPF_TRY(tsmm(ctx, n, r, 1, Zc, 0, Rinv, 0, 1.0, nullptr, 0.0, Cc, nullptr));
+        const int blocks = std::max(1, std::min(ceil_div((long long)np, 256), ctx->num_sms * 8));
+        // Q_C's columns from the Cholesky-QR; the dropped ones become zero columns
+        pad_cols_kernel<<<blocks, 256, 0, ctx->stream>>>(n, r, p, Qc, dfl.Qp);
+        BPF_LAUNCHED(ctx);
+        if (r_ok < r) {
+            zero_cols_kernel<<<blocks, 256, 0, ctx->stream>>>(n, r_ok, r, p, dfl.Qp);
+            BPF_LAUNCHED(ctx);
+        }
+        pad_cols_kernel<<<blocks, 256, 0, ctx->stream>>>(n, r, p, Cc, dfl.Zp);
+        BPF_LAUNCHED(ctx);
+        if (r_ok == 0) dfl.r = 0;
+        // keep the Cholesky-QR's retained R (its last pass) consistent: the solve only needs
+        // Q_C and Zd, which satisfy A Zd = Q_C up to rounding
+    }
     gmres_init_kernel<<<1, 1, 0, ctx->stream>>>(st, opts->atol, opts->rtol, hist, timemax - (now_s() - t0));
     BPF_LAUNCHED(ctx);
     BPF_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(SolveState), cudaMemcpyDeviceToHost, ctx->stream));
@@ -259,6 +349,11 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
                 BPF_TRY(spmm_rowmajor(ctx, n, A->nnz, rp, ci, av, base, p, 1.0, Xi, 0.0, W, Bi));
                 if (M) BPF_TRY(prec_apply_rowmajor(ctx, M, p, W, Qm));
             }
+        }
+        if (dfl.r > 0) {   // R0 -= Q_C (Q_C^T R0), Xdef = Zd (Q_C^T R0)
+            BPF_TRY(gram(ctx, n, p, 1, dfl.Qp, 0, R0, dfl.E2, 1.0, false, st));
+            BPF_TRY(tsmm(ctx, n, p, 1, dfl.Qp, 0, dfl.E2, 0, -1.0, R0, 1.0, R0, st));
+            BPF_TRY(tsmm(ctx, n, p, 1, dfl.Zp, 0, dfl.E2, 0, 1.0, nullptr, 0.0, dfl.Xdef, st));
         }
         BPF_TRY(cholqr(ctx, n, p, R0, g.V, g.Z, Tq, st));                    // :275-276
         npass++;
@@ -294,8 +389,17 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
                     Qk = Qm;
                 }
                 double *Psi = g.Rblk + rblk_pos(0, jj) * pp;                     // :301-313
+                double *Ek = dfl.r > 0 ? dfl.E + (size_t)jj * pp : nullptr;
+                if (Ek) {   // against Q_C first (GCRO): E_k = Q_C^T W, W -= Q_C E_k
+                    BPF_TRY(gram(ctx, n, p, 1, dfl.Qp, 0, Qk, Ek, 1.0, false, st));
+                    BPF_TRY(tsmm(ctx, n, p, 1, dfl.Qp, 0, Ek, 0, -1.0, Qk, 1.0, Qk, st));
+                }
                 BPF_TRY(gram(ctx, n, p, kk, g.V, np, Qk, Psi, 1.0, false, st));
                 BPF_TRY(tsmm(ctx, n, p, kk, g.V, np, Psi, pp, -1.0, Qk, 1.0, Qk, st));
+                if (Ek) {
+                    BPF_TRY(gram(ctx, n, p, 1, dfl.Qp, 0, Qk, Ek, 1.0, true, st, nullptr, dfl.E2));
+                    BPF_TRY(tsmm(ctx, n, p, 1, dfl.Qp, 0, dfl.E2, 0, -1.0, Qk, 1.0, Qk, st));
+                }
                 BPF_TRY(gram(ctx, n, p, kk, g.V, np, Qk, Psi, 1.0, true, st, nullptr, Psi2buf));
                 BPF_TRY(tsmm(ctx, n, p, kk, g.V, np, Psi2buf, pp, -1.0, Qk, 1.0, Qk, st));
                 double *Cm = Cpar[kk & 1];
@@ -362,6 +466,11 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
             BPF_CUDA(ctx, cudaMemcpyAsync(Pm, Xr, sizeof(double) * np, cudaMemcpyDeviceToDevice, ctx->stream));
             BPF_TRY(prec_apply_rowmajor(ctx, N, p, Pm, Xr));
         }
+        if (dfl.r > 0 && inner_iter > 0) {   // x = x0' + N^{-1} V y - Zd (E y)
+            BPF_TRY(tsmm(ctx, p, p, inner_iter, dfl.E, pp, Yb, pp, 1.0, nullptr, 0.0, dfl.F, nullptr));
+            BPF_TRY(tsmm(ctx, n, p, 1, dfl.Zp, 0, dfl.F, 0, -1.0, dfl.Xdef, 1.0, dfl.Xdef, nullptr));
+        }
+        if (dfl.r > 0) BPF_TRY(axpby(ctx, np, 1.0, dfl.Xdef, 1.0, Xr, nullptr));
         if (restart) BPF_TRY(axpby(ctx, np, 1.0, dX, 1.0, Xi, nullptr));
         inner_itmax -= inner_iter;                                          // :388-392
         iter += inner_iter;
@@ -391,4 +500,20 @@ extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p
     if (opts->verbose > 0) printf("\n");
     stats->timer = now_s() - t0;
     return BPF_SUCCESS;
+}
+
+extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p, const double *B,
+                                      int ldb, double *X, int ldx, const double *X0, int ldx0,
+                                      const bpf_prec *M, const bpf_prec *N, const bpf_gmres_opts *opts,
+                                      bpf_stats *stats) {
+    return block_gmres_impl(ctx, A, p, B, ldb, X, ldx, X0, ldx0, M, N, opts, stats, nullptr, 0, 0);
+}
+
+extern "C" bpf_status bpf_block_gmres_deflated(bpf_ctx *ctx, const bpf_csr_desc *A, int p,
+                                               const double *B, int ldb, double *X, int ldx,
+                                               const double *X0, int ldx0, const bpf_prec *M,
+                                               const bpf_prec *N, const bpf_gmres_opts *opts,
+                                               const double *Z, int ldz, int rank, bpf_stats *stats) {
+    if (rank < 0) return set_error(ctx, BPF_ERR_INVALID_VALUE, "block_gmres: negative deflation rank");
+    return block_gmres_impl(ctx, A, p, B, ldb, X, ldx, X0, ldx0, M, N, opts, stats, Z, ldz, rank);
 }

@@ -160,6 +160,45 @@ BPF_API bpf_status bpf_tc_gemm_bf16(bpf_ctx *ctx, int M, int N, int K, const voi
                                     const void *B, int ldb, float *D, int ldd, int accumulate,
                                     int splits);
 
+/* ---- learned warm start and deflation basis -----------------------------------------------
+ * No counterpart in the reference: a 3-layer MLP (n -> hidden -> hidden -> n, LeakyReLU 0.25,
+ * BF16 weights with FP32 masters, tensor-core products, Adam) that maps a right-hand side b to
+ * a warm start x0 = s ||b|| f(b / ||b||) for block-GMRES and spans a low-rank deflation basis.
+ * It is trained on the solver's own (b, x) pairs; the solver then runs from x0 to the requested
+ * residual, so a poor network costs iterations, never accuracy.  All pointers are device
+ * pointers, blocks column-major; batches of at most 128 columns for the training calls. */
+typedef struct bpf_mlp bpf_mlp;
+BPF_API bpf_status bpf_mlp_create(bpf_ctx *ctx, int n, int hidden, unsigned long long seed,
+                                  bpf_mlp **mlp);
+BPF_API bpf_status bpf_mlp_destroy(bpf_mlp *mlp);
+/* s: the output scale (the training set's typical ||x|| / ||b||). */
+BPF_API bpf_status bpf_mlp_set_scale(bpf_mlp *mlp, double scale);
+/* X (n x p) = warm starts for the columns of B (n x p), any p. */
+BPF_API bpf_status bpf_mlp_forward(bpf_mlp *mlp, int p, const double *B, int ldb, double *X,
+                                   int ldx);
+/* Loss L = (1/p) sum_j ||y_j - t_j||^2 / ||t_j||^2 (t_j = x_j / (s ||b_j||)) of the batch
+ * (B, X), p <= 128, and its gradients in the parameters' gradient buffers (bpf_mlp_params);
+ * *loss (host, nullable) receives L. */
+BPF_API bpf_status bpf_mlp_gradients(bpf_mlp *mlp, int p, const double *B, int ldb,
+                                     const double *X, int ldx, double *loss);
+/* bpf_mlp_gradients followed by one Adam step (beta 0.9 / 0.999) with learning rate lr. */
+BPF_API bpf_status bpf_mlp_train_step(bpf_mlp *mlp, int p, const double *B, int ldb,
+                                      const double *X, int ldx, double lr, double *loss);
+/* Device FP32 parameter `which` (0 W1 [hidden x np], 1 b1, 2 W2 [hidden x hidden], 3 b2,
+ * 4 W3 [np x hidden], 5 b3 [np]; np = n rounded up to 128, padding zero), its gradient buffer
+ * and shape.  After writing parameters, call bpf_mlp_refresh. */
+BPF_API bpf_status bpf_mlp_params(bpf_mlp *mlp, int which, float **w, float **grad,
+                                  long long *rows, long long *cols);
+BPF_API bpf_status bpf_mlp_refresh(bpf_mlp *mlp);
+/* Copy parameter `which` (or its gradient, grad = 1) to the device buffer buf (to_network = 0)
+ * or from it into the network (to_network = 1; refreshes the BF16 copies). */
+BPF_API bpf_status bpf_mlp_param_copy(bpf_mlp *mlp, int which, int grad, float *buf,
+                                      int to_network);
+/* Z (n x rank) = an orthonormal basis of the network's outputs on rank seeded Gaussian
+ * probes (the span it has learned), for deflated block-GMRES. */
+BPF_API bpf_status bpf_mlp_basis(bpf_mlp *mlp, int rank, unsigned long long seed, double *Z,
+                                 int ldz);
+
 /* ---- sparse x dense block -------------------------------------------------------------- */
 /* Y = alpha*A*X + beta*Y: mul!(W, A, P) of src/block_gmres.jl:299 (CSR SpMM). */
 BPF_API bpf_status bpf_spmm(bpf_ctx *ctx, const bpf_csr_desc *A, int p, double alpha,
@@ -227,6 +266,18 @@ BPF_API bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p,
                                    const double *X0, int ldx0, const bpf_prec *M,
                                    const bpf_prec *N, const bpf_gmres_opts *opts,
                                    bpf_stats *stats);
+/* block_gmres with a deflation basis Z (n x rank device block, column-major, rank <= p): the
+ * GCRO form of Krylov-subspace augmentation -- Q_C = orthonormalized A Z, the starting residual
+ * projected off Q_C, every new block orthogonalized against Q_C before the basis, and
+ * x = x0 + Z R^{-1} Q_C^T r0 + N \ V y - Z R^{-1} E y.  Same options, stopping rule (epsilon from
+ * the unprojected initial residual) and statistics as bpf_block_gmres; right preconditioning
+ * only.  No counterpart in the reference: the learned deflation basis of bpf_mlp_basis is its
+ * intended input (any basis works; the solver still reaches the requested residual). */
+BPF_API bpf_status bpf_block_gmres_deflated(bpf_ctx *ctx, const bpf_csr_desc *A, int p,
+                                            const double *B, int ldb, double *X, int ldx,
+                                            const double *X0, int ldx0, const bpf_prec *M,
+                                            const bpf_prec *N, const bpf_gmres_opts *opts,
+                                            const double *Z, int ldz, int rank, bpf_stats *stats);
 
 /* block_bicgstab(A, B; C=B, N, kwargs...) -> (X, stats): src/block_bicgstab.jl:182-299.
  * C (shadow block) nullable -> B.  N: right preconditioner (nullable = I), applied as
