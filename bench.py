@@ -42,9 +42,11 @@ N_BUS, N_PV, P_RHS = 9000, 1000, 64
 RTOL = 1e-8
 ITMAX = 300
 CPU_SAMPLE_ITERS = (4, 10)
-# DRAM bytes (read + write) per launch of each kernel class, from one ncu capture of the
-# benchmark's solve (profiles/launches_grid9k_p64.md); None where not captured.
-TRAFFIC_PER_LAUNCH = {}
+# DRAM bytes (read + write) per working launch of the FP64 product classes in the benchmark's
+# solve (minimum-degree ILU(0), 57 iterations), from one ncu capture of every launch
+# (profiles/launches_grid9k_p64_amd_ilu0_gmres.md): the kernels' total DRAM bytes over the
+# launches that always do their work, the ones bench.py's per-class timing counts.
+TRAFFIC_PER_LAUNCH = {"gram": 135.58e6, "tsmm": 126.28e6}
 
 
 def peaks():
@@ -200,7 +202,7 @@ def workload_config(world):
             "parallelism": f"replicas x{world} (independent grids)"}
 
 
-def kernel_only(name, reps, iters=24):
+def kernel_only(name, reps, iters=24, ordering="natural"):
     """A few launches of one kernel on a case whose blocks exceed L2, for ncu captures:
     70,000-bus grid (134,998 unknowns, ~980k nonzeros), 128 right-hand sides."""
     import numpy as np
@@ -214,13 +216,28 @@ def kernel_only(name, reps, iters=24):
         J, B = make_workload(0)
         A = bpf.CuSparseMatrixCSR.from_scipy(J)
         Bd = bpf.colmajor(torch.as_tensor(B, device="cuda"))
-        N = bpf.ilu0(A, P_RHS)
+        N = bpf.ilu0(A, P_RHS, ordering=ordering)
         for _ in range(reps):
             X, st = bpf.block_gmres(A, Bd, N=N, ldiv=True, restart=False, memory=ITMAX, atol=0.0,
                                     rtol=RTOL, itmax=iters)
         torch.cuda.synchronize()
         print(json.dumps({"kernel_only": name, "n": J.shape[0], "p": P_RHS, "reps": reps,
                           "iterations": st.niter}))
+        return
+    if name == "mlp":
+        # training steps of the learned warm start on the benchmark's grid (16,998 unknowns,
+        # hidden 512, batches of 64 solver-style pairs): the tcgen05 GEMMs of forward + backward
+        from blockpowerflow_b200 import learned
+
+        J, B = make_workload(0)
+        n = J.shape[0]
+        mlp = learned.WarmStartMLP(n, 512, seed=0)
+        Bd = bpf.colmajor(torch.as_tensor(B, device="cuda"))
+        Xd = bpf.colmajor(torch.randn(n, P_RHS, dtype=torch.float64, device="cuda"))
+        for _ in range(reps):
+            loss = mlp.train_step(Bd, Xd, 1e-4)
+        torch.cuda.synchronize()
+        print(json.dumps({"kernel_only": name, "n": n, "p": P_RHS, "reps": reps, "loss": loss}))
         return
     J = bpf.grid.preset_jacobian("case70k", 0)
     n = J.shape[0]
@@ -426,10 +443,11 @@ def config_bicgstab9k(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel-only", choices=["trsv", "spmm", "factor", "gram", "gmres"], default=None,
+    ap.add_argument("--kernel-only", choices=["trsv", "spmm", "factor", "gram", "gmres", "mlp"], default=None,
                     help="launch one kernel a few times on a 135k-unknown case (for ncu)")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--iters", type=int, default=24, help="block-GMRES iterations (--kernel-only gmres)")
+    ap.add_argument("--ordering", default="natural", help="ILU(0) ordering (--kernel-only gmres)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -446,7 +464,7 @@ def main():
          "rf25k": config_rf25k}[args.config](args)
         return
     if args.kernel_only:
-        kernel_only(args.kernel_only, args.reps, args.iters)
+        kernel_only(args.kernel_only, args.reps, args.iters, args.ordering)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
