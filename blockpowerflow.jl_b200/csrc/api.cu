@@ -176,6 +176,75 @@ bpf_status prec_setup(bpf_ctx *ctx, int kind, int n, const std::vector<int> &rp,
     up_i(&P->pp, pp);
     up_i(&P->pdst, pdst);
     up_i(&P->psrc, psrc);
+    if (kind == PREC_LU && n > 0) {
+        // column-step levels: step k depends on the steps j < k with L(k, j) != 0 (they update
+        // row k) or U(j, k) != 0 (they update column k)
+        std::vector<int> lev(n, 0);
+        std::vector<std::vector<int>> ucol(n);   // ucol[k]: rows j < k with U(j, k) != 0
+        for (int j = 0; j < n; j++)
+            for (int q = diag[j] + 1; q < rp[j + 1]; q++) ucol[ci[q]].push_back(j);
+        int nlev = 0;
+        for (int k = 0; k < n; k++) {
+            int l = 0;
+            for (int q = rp[k]; q < diag[k]; q++) l = std::max(l, lev[ci[q]] + 1);
+            for (int j : ucol[k]) l = std::max(l, lev[j] + 1);
+            lev[k] = l;
+            nlev = std::max(nlev, l + 1);
+            std::vector<int>().swap(ucol[k]);
+        }
+        std::vector<int> lptr(nlev + 1, 0), ent;
+        for (int i = 0; i < n; i++)
+            for (int q = rp[i]; q < diag[i]; q++) lptr[lev[ci[q]] + 1]++;
+        for (int l = 0; l < nlev; l++) lptr[l + 1] += lptr[l];
+        ent.resize(lptr[nlev]);
+        std::vector<int> fill(lptr.begin(), lptr.end() - 1);
+        for (int i = 0; i < n; i++)
+            for (int q = rp[i]; q < diag[i]; q++) ent[fill[lev[ci[q]]]++] = q;
+        int mx = 0;
+        for (int l = 0; l < nlev; l++) mx = std::max(mx, lptr[l + 1] - lptr[l]);
+        P->cl_nlev = nlev;
+        P->cl_max_level = mx;
+        up_i(&P->cl_lev_ptr, lptr);
+        up_i(&P->cl_ent, ent);
+        // push lists of the two sweeps: forward, L entry (i, k) leaves row k (level of k in
+        // the forward sweep) for row i; backward, U entry (i, k), i < k, leaves row k for row i
+        int pmx = 0;
+        for (int sweep = 0; sweep < 2; sweep++) {
+            const TriHost &t = sweep == 0 ? lo : up;
+            std::vector<int> lv(n, 0);
+            for (int l = 0; l < t.nlev; l++)
+                for (int q = t.lev_ptr[l]; q < t.lev_ptr[l + 1]; q++) lv[t.rows[q]] = l;
+            std::vector<int> ptr(t.nlev + 1, 0);
+            for (int i = 0; i < n; i++)
+                for (int q = rp[i]; q < rp[i + 1]; q++) {
+                    const int k = ci[q];
+                    if (sweep == 0 ? (k < i) : (k > i)) ptr[lv[k] + 1]++;
+                }
+            for (int l = 0; l < t.nlev; l++) {
+                pmx = std::max(pmx, ptr[l + 1]);
+                ptr[l + 1] += ptr[l];
+            }
+            std::vector<int> src(ptr[t.nlev]), dst(ptr[t.nlev]), pos(ptr[t.nlev]);
+            std::vector<int> fl(ptr.begin(), ptr.end() - 1);
+            for (int i = 0; i < n; i++)
+                for (int q = rp[i]; q < rp[i + 1]; q++) {
+                    const int k = ci[q];
+                    if (sweep == 0 ? (k < i) : (k > i)) {
+                        const int w = fl[lv[k]]++;
+                        src[w] = k;
+                        dst[w] = i;
+                        pos[w] = q;
+                    }
+                }
+            P->ps_nlev[sweep] = t.nlev;
+            up_i(&P->ps_ptr[sweep], ptr);
+            up_i(&P->ps_src[sweep], src);
+            up_i(&P->ps_dst[sweep], dst);
+            up_i(&P->ps_pos[sweep], pos);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        }
+        P->ps_max_level = pmx;
+    }
     if (e == cudaSuccess && nnz > 0) e = cudaMalloc((void **)&P->fv, sizeof(double) * nnz);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // host vectors die on return
     if (e != cudaSuccess) return fail(cuda_error(ctx, e, "preconditioner setup", __FILE__, __LINE__));
@@ -497,6 +566,14 @@ bpf_status bpf_prec_destroy(bpf_prec *P) {
     cudaFree(P->perm);
     cudaFree(P->amap);
     cudaFree(P->zbuf);
+    cudaFree(P->cl_lev_ptr);
+    cudaFree(P->cl_ent);
+    for (int w = 0; w < 2; w++) {
+        cudaFree(P->ps_ptr[w]);
+        cudaFree(P->ps_src[w]);
+        cudaFree(P->ps_dst[w]);
+        cudaFree(P->ps_pos[w]);
+    }
     delete P;
     return BPF_SUCCESS;
 }

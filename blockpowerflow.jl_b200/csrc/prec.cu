@@ -329,6 +329,90 @@ __global__ void __launch_bounds__(256) factor_coop_kernel(FactorArgs a) {
     }
 }
 
+// Right-looking LU on a fill pattern by column steps (the RF refactorization).  Level by
+// level, a warp per L entry e = (i, k) of the level's steps: l_ik = a_ik / u_kk, then the
+// entry's update pairs a_ij -= l_ik u_kj, added atomically (independent steps of one level may
+// update the same entry).  Every value a level reads was final before its barrier.
+__global__ void __launch_bounds__(256) lu_colstep_kernel(int nlev, const int *__restrict__ lev_ptr,
+                                                         const int *__restrict__ ent, const int *__restrict__ ci,
+                                                         const int *__restrict__ diag, const int *__restrict__ pp,
+                                                         const int *__restrict__ pdst, const int *__restrict__ psrc,
+                                                         double *fv, DevStatus *ds) {
+    __shared__ unsigned s_gen;
+    if (threadIdx.x == 0) s_gen = barrier_gen_start(ds);
+    __syncthreads();
+    unsigned gen = s_gen;
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    for (int l = 0; l < nlev; l++) {
+        const int q0 = __ldg(lev_ptr + l), q1 = __ldg(lev_ptr + l + 1);
+        for (int q = q0 + gw; q < q1; q += nw) {
+            const int e = __ldg(ent + q);
+            const int k = __ldg(ci + e);
+            double lik = 0.0;
+            if (lane == 0) {
+                const double piv = __ldcg(fv + __ldg(diag + k));
+                if (piv == 0.0) {
+                    if (atomicCAS(&ds->err, 0, (int)DEV_ZERO_PIVOT) == 0) ds->aux = k;
+                } else {
+                    lik = __ldcg(fv + e) / piv;
+                }
+                fv[e] = lik;
+            }
+            lik = __shfl_sync(0xffffffffu, lik, 0);
+            const int t1 = __ldg(pp + e + 1);
+            if (lik != 0.0)
+                for (int t = __ldg(pp + e) + lane; t < t1; t += 32)
+                    atomicAdd(fv + __ldg(pdst + t), -lik * __ldcg(fv + __ldg(psrc + t)));
+        }
+        if (l + 1 < nlev) {
+            if (!grid_barrier(ds, gen)) return;
+        }
+    }
+}
+
+// LU solve in push form, in place on row-major n x p blocks (p <= 256): forward sweep, level by
+// level, a warp per unit-L entry (i, k) whose source row k is final: y_i -= l_ik y_k; backward
+// sweep, a warp per U entry (i, k), i < k: y_i -= (u_ik / u_kk) y_k with y_k not yet divided;
+// finally y_k /= u_kk.  Rows of a level receive atomic contributions from many entries at once,
+// so a level's work is spread over all the factor entries, not over its (few, long) rows.
+__global__ void __launch_bounds__(512) lu_push_solve_kernel(int n, int p, int nlev0, const int *__restrict__ ptr0,
+                                                            const int *__restrict__ src0, const int *__restrict__ dst0,
+                                                            const int *__restrict__ pos0, int nlev1,
+                                                            const int *__restrict__ ptr1, const int *__restrict__ src1,
+                                                            const int *__restrict__ dst1, const int *__restrict__ pos1,
+                                                            const int *__restrict__ diag, const double *__restrict__ fv,
+                                                            double *Y, DevStatus *ds) {
+    __shared__ unsigned s_gen;
+    if (threadIdx.x == 0) s_gen = barrier_gen_start(ds);
+    __syncthreads();
+    unsigned gen = s_gen;
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    for (int sweep = 0; sweep < 2; sweep++) {
+        const int nlev = sweep == 0 ? nlev0 : nlev1;
+        const int *ptr = sweep == 0 ? ptr0 : ptr1, *src = sweep == 0 ? src0 : src1,
+                  *dst = sweep == 0 ? dst0 : dst1, *pos = sweep == 0 ? pos0 : pos1;
+        for (int l = 0; l < nlev; l++) {
+            const int q0 = __ldg(ptr + l), q1 = __ldg(ptr + l + 1);
+            for (int q = q0 + gw; q < q1; q += nw) {
+                const int k = __ldg(src + q), i = __ldg(dst + q);
+                double a = __ldg(fv + __ldg(pos + q));
+                if (sweep == 1) a /= __ldg(fv + __ldg(diag + k));
+                const double *yk = Y + (size_t)k * p;
+                double *yi = Y + (size_t)i * p;
+                for (int c = lane; c < p; c += 32) atomicAdd(yi + c, -a * __ldcg(yk + c));
+            }
+            if (!grid_barrier(ds, gen)) return;
+        }
+    }
+    const size_t total = (size_t)n * p;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x)
+        Y[e] = __ldcg(Y + e) / __ldg(fv + __ldg(diag + e / p));
+}
+
 // Cooperative grid size: enough blocks for the widest level, capped by co-residency.
 template <typename K>
 static bpf_status coop_grid(bpf_ctx *ctx, K kernel, int threads, size_t smem, int want,
@@ -342,6 +426,25 @@ static bpf_status coop_grid(bpf_ctx *ctx, K kernel, int threads, size_t smem, in
 }
 
 bpf_status factor_numeric(bpf_ctx *ctx, bpf_prec *P) {
+    if (P->kind == PREC_LU && P->cl_nlev > 0) {
+        int grid = 1;
+        BPF_TRY(coop_grid(ctx, lu_colstep_kernel, 256, 0, std::max(1, ceil_div(P->cl_max_level, 8)), &grid));
+        int nlev = P->cl_nlev;
+        const int *lp = P->cl_lev_ptr, *en = P->cl_ent, *ci = P->ci, *dg = P->diag, *pp = P->pp,
+                  *pd = P->pdst, *ps = P->psrc;
+        double *fv = P->fv;
+        DevStatus *ds = ctx->dstat;
+        void *args[] = {&nlev, (void *)&lp, (void *)&en, (void *)&ci, (void *)&dg, (void *)&pp,
+                        (void *)&pd, (void *)&ps, &fv, &ds};
+        // Algorithmic bytes: the factor values read and written once, the entry list, and per
+        // update pair two indices, one value read and one atomically updated.
+        KScope ks(ctx, BPF_KC_FACTOR, 16.0 * P->nnz + 8.0 * (P->n + 1) + 24.0 * P->npairs,
+                  2.0 * P->npairs);
+        BPF_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)lu_colstep_kernel, dim3(grid), dim3(256),
+                                                  args, 0, ctx->stream));
+        BPF_LAUNCHED(ctx);
+        return BPF_SUCCESS;
+    }
     FactorArgs a;
     a.n = P->n;
     a.rp = P->rp;
@@ -550,6 +653,31 @@ bpf_status prec_load_values(bpf_ctx *ctx, bpf_prec *P, const double *vals) {
     }
     const int blocks = std::max(1, std::min(ceil_div(P->nnz, 256), ctx->num_sms * 8));
     scatter_map_kernel<<<blocks, 256, 0, ctx->stream>>>(P->nnz, vals, P->amap, P->fv);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
+bpf_status lu_solve_push_rowmajor(bpf_ctx *ctx, const bpf_prec *P, int p, double *Y) {
+    if (P->n == 0 || p == 0) return BPF_SUCCESS;
+    if (p > 256) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "LU solve: p=%d > 256 per call", p);
+    int grid = 1;
+    BPF_TRY(coop_grid(ctx, lu_push_solve_kernel, 512, 0,
+                      std::min(ctx->num_sms * 2, std::max(1, ceil_div(P->ps_max_level, 16))), &grid));
+    int n = P->n, nl0 = P->ps_nlev[0], nl1 = P->ps_nlev[1];
+    const int *p0 = P->ps_ptr[0], *s0 = P->ps_src[0], *d0 = P->ps_dst[0], *q0 = P->ps_pos[0];
+    const int *p1 = P->ps_ptr[1], *s1 = P->ps_src[1], *d1 = P->ps_dst[1], *q1 = P->ps_pos[1];
+    const int *dg = P->diag;
+    const double *fv = P->fv;
+    DevStatus *ds = ctx->dstat;
+    void *args[] = {&n, &p, &nl0, (void *)&p0, (void *)&s0, (void *)&d0, (void *)&q0, &nl1, (void *)&p1,
+                    (void *)&s1, (void *)&d1, (void *)&q1, (void *)&dg, (void *)&fv, &Y, &ds};
+    // Algorithmic bytes: per factor entry 3 indices and its value, the block read once per
+    // entry's source row and target row updated (atomics), read and written once at the end.
+    const double nnz_off = (double)P->nnz - P->n;
+    KScope ks(ctx, BPF_KC_TRSV, 20.0 * nnz_off + 8.0 * P->n + 32.0 * (double)P->n * p,
+              2.0 * (nnz_off + P->n) * p);
+    BPF_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)lu_push_solve_kernel, dim3(grid), dim3(512), args, 0,
+                                              ctx->stream));
     BPF_LAUNCHED(ctx);
     return BPF_SUCCESS;
 }

@@ -85,6 +85,16 @@ struct bpf_prec {
     long long npairs = 0;
     bpf::TriDev lower;   // forward solve (L unit for ILU0; L for IC0)
     bpf::TriDev upper;   // backward solve (U for ILU0; L' for IC0)
+    // LU on a fill pattern (the RF refactorization): right-looking column steps; step k (scale
+    // column k of L by 1 / u_kk, then apply its update pairs) waits for the steps that update
+    // row k or column k.  cl_lev_ptr / cl_ent: the L entries of each level's steps.
+    int cl_nlev = 0, cl_max_level = 0;
+    int *cl_lev_ptr = nullptr, *cl_ent = nullptr;
+    // LU solves in push form (right-looking): per level of each sweep, the factor entries whose
+    // source row became final at that level, as (source row, target row, position in fv).
+    int ps_nlev[2] = {0, 0}, ps_max_level = 0;
+    int *ps_ptr[2] = {nullptr, nullptr}, *ps_src[2] = {nullptr, nullptr},
+        *ps_dst[2] = {nullptr, nullptr}, *ps_pos[2] = {nullptr, nullptr};
     // Symmetric reordering (bpf_ilu0_create_ordered): the factors are those of A_hat =
     // A(perm, perm); perm[i] = original row of factor row i; amap[k] = position of A's entry
     // k in A_hat's pattern; zbuf = n x zcols factor-ordered scratch of the solves.
@@ -108,4 +118,6 @@ bpf_status prec_apply_rowmajor(bpf_ctx *ctx, const bpf_prec *P, int p, const dou
 bpf_status prec_reserve_z(bpf_ctx *ctx, bpf_prec *P, int p);
 // A's values into the factor storage (a copy, or the scatter through amap when reordered).
 bpf_status prec_load_values(bpf_ctx *ctx, bpf_prec *P, const double *vals);
+// Y = U^{-1} L^{-1} Y in place (row-major n x p, p <= 256) for an LU factor with push lists.
+bpf_status lu_solve_push_rowmajor(bpf_ctx *ctx, const bpf_prec *P, int p, double *Y);
 }  // namespace bpf

@@ -393,7 +393,10 @@ bpf_status bpf_rf_solve(bpf_rf *rf, int nrhs, double *X, int ldx) {
         for (int c0 = 0; c0 < nrhs; c0 += chunk) {
             int pc = std::min(chunk, nrhs - c0);
             BPF_TRY(conv_in(c0, pc));
-            BPF_TRY(prec_apply_rowmajor(ctx, rf->lu, pc, buf, buf));
+            if (rf->lu->ps_nlev[0] + rf->lu->ps_nlev[1] > 0)
+                BPF_TRY(lu_solve_push_rowmajor(ctx, rf->lu, pc, buf));
+            else
+                BPF_TRY(prec_apply_rowmajor(ctx, rf->lu, pc, buf, buf));
             BPF_TRY(conv_out(c0, pc));
         }
         return BPF_SUCCESS;
