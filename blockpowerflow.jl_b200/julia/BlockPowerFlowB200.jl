@@ -158,7 +158,8 @@ function block_gmres(A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64},
                      X0::Union{Nothing,CuMatrix{Float64}}=nothing; memory::Int=20, M=I, N=I,
                      ldiv::Bool=false, restart::Bool=false, reorthogonalization::Bool=false,
                      atol::Float64=√eps(Float64), rtol::Float64=√eps(Float64), itmax::Int=0,
-                     timemax::Float64=Inf, verbose::Int=0, history::Bool=false)
+                     timemax::Float64=Inf, verbose::Int=0, history::Bool=false,
+                     deflation::Union{Nothing,CuMatrix{Float64}}=nothing)
     n, p = size(B)
     size(A, 1) == size(A, 2) || error("System must be square")
     size(A, 1) == n || error("Inconsistent problem size")
@@ -170,11 +171,22 @@ function block_gmres(A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64},
     st = Ref(CStats(0, 0, 0, 0.0, 0, cap, pointer(res), 0))
     x0p = X0 === nothing ? CU_NULL : pointer(X0)
     GC.@preserve res begin
-        check(ccall((:bpf_block_gmres, libbpf), Cint,
-                    (Ptr{Cvoid}, Ref{CsrDesc}, Cint, CuPtr{Cdouble}, Cint, CuPtr{Cdouble}, Cint,
-                     CuPtr{Cdouble}, Cint, Ptr{Cvoid}, Ptr{Cvoid}, Ref{GmresOpts}, Ref{CStats}),
-                    ctx(), Ref(desc(A)), p, pointer(B), stride(B, 2), pointer(X), stride(X, 2),
-                    x0p, n, _handle(M), _handle(N), opts, st))
+        if deflation === nothing
+            check(ccall((:bpf_block_gmres, libbpf), Cint,
+                        (Ptr{Cvoid}, Ref{CsrDesc}, Cint, CuPtr{Cdouble}, Cint, CuPtr{Cdouble}, Cint,
+                         CuPtr{Cdouble}, Cint, Ptr{Cvoid}, Ptr{Cvoid}, Ref{GmresOpts}, Ref{CStats}),
+                        ctx(), Ref(desc(A)), p, pointer(B), stride(B, 2), pointer(X), stride(X, 2),
+                        x0p, n, _handle(M), _handle(N), opts, st))
+        else   # an addition: GCRO deflation with an n x rank basis (rank <= p)
+            size(deflation, 1) == n || error("Inconsistent deflation basis size")
+            check(ccall((:bpf_block_gmres_deflated, libbpf), Cint,
+                        (Ptr{Cvoid}, Ref{CsrDesc}, Cint, CuPtr{Cdouble}, Cint, CuPtr{Cdouble}, Cint,
+                         CuPtr{Cdouble}, Cint, Ptr{Cvoid}, Ptr{Cvoid}, Ref{GmresOpts},
+                         CuPtr{Cdouble}, Cint, Cint, Ref{CStats}),
+                        ctx(), Ref(desc(A)), p, pointer(B), stride(B, 2), pointer(X), stride(X, 2),
+                        x0p, n, _handle(M), _handle(N), opts, pointer(deflation),
+                        stride(deflation, 2), size(deflation, 2), st))
+        end
     end
     s = st[]
     stats = BlockGMRESStats{Float64}(s.niter, s.solved != 0,
