@@ -441,6 +441,134 @@ def config_bicgstab9k(args):
     print(json.dumps(line), flush=True)
 
 
+def batch_workload(nsys=512, seed=0):
+    """Fourth configuration's inputs: nsys synthetic grids with log-uniform 100 - 3,000 buses
+    and U{8..64} Gaussian right-hand sides each (seeded)."""
+    import numpy as np
+
+    from blockpowerflow_b200 import grid as g
+
+    rng = np.random.default_rng(seed)
+    buses = np.exp(rng.uniform(np.log(100), np.log(3000), nsys)).astype(int)
+    nrhs = rng.integers(8, 65, nsys)
+    mats = [g.jacobian(g.make_grid(int(b), seed=1000 + k)).tocsr() for k, b in enumerate(buses)]
+    Bs = [g.gaussian_rhs(A.shape[0], int(p), 5000 + k) for k, (A, p) in enumerate(zip(mats, nrhs))]
+    return buses, [int(p) for p in nrhs], mats, Bs
+
+
+def config_batch512(args):
+    """Fourth configuration: 512 independent grids (100 - 3,000 buses, log-uniform), 8 - 64
+    RHS each, ILU(0) block-GMRES in one persistent CUDA-graph launch (FP32 factors, FP64
+    residual and orthogonalization), launch shape chosen by the autotuner.  One step = the
+    ILU(0) of every system + the solve of every right-hand side (one graph launch).  Beside it:
+    the plain FP64 drop-in (bpf.ilu0 + bpf.block_gmres per system, natural order, one system
+    after another) on the same inputs, and the oracle on a sample of the systems."""
+    import numpy as np
+    import torch
+
+    import blockpowerflow_b200 as bpf
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    nsys = int(os.environ.get("BPF_BATCH_NSYS", "512"))
+    buses, nrhs, mats, Bs = batch_workload(nsys)
+    total_rhs = int(sum(nrhs))
+    dm = [bpf.CuSparseMatrixCSR.from_scipy(A) for A in mats]
+    Bd = [torch.as_tensor(B, device="cuda") for B in Bs]
+    t0 = time.time()
+    tune = bpf.autotune(dm, nrhs, Bd, cache_path=os.environ.get("BPF_TUNE_CACHE"), repeats=1)
+    t_tune = time.time() - t0
+    t0 = time.time()
+    plan = bpf.BatchPlan(dm, nrhs, slice=tune["slice"], ctas_per_sm=tune["ctas_per_sm"])
+    torch.cuda.synchronize()
+    t_plan = time.time() - t0
+    for _ in range(max(3, args.warmup)):
+        Xs, st = plan.solve(Bd)
+    torch.cuda.synchronize()
+    worst = 0.0
+    for A, B, X in zip(mats, Bs, Xs):
+        worst = max(worst, float(np.linalg.norm(B - A @ X.cpu().numpy()) / np.linalg.norm(B)))
+    solved = all(x.solved for x in st)
+    units = plan.unit_stats()
+    cyc = plan.unit_cycles()
+    steps = max(args.steps, 5)
+    launches0 = bpf.kernel_launches()
+    bpf._lib.set_timing(True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        Xs, st = plan.solve(Bd)
+    e1.record()
+    torch.cuda.synchronize()
+    t_ms = e0.elapsed_time(e1)
+    launches = bpf.kernel_launches() - launches0
+    ms_b, cnt_b, by_b, fl_b = bpf._lib.kernel_time("batch")
+    bpf._lib.set_timing(False)
+    # end to end: host (pinned) B in, X out, through the public API
+    Bh = [torch.as_tensor(B).pin_memory() for B in Bs]
+    h2d = sum(B.numel() * 8 for B in Bh)
+    torch.cuda.synchronize()
+    te = time.time()
+    e_steps = max(2, steps // 2)
+    for _ in range(e_steps):
+        Xs_e, _ = plan.solve([B.to("cuda", non_blocking=True) for B in Bh])
+        Xh = [X.cpu() for X in Xs_e]
+    torch.cuda.synchronize()
+    t_e2e = (time.time() - te) / e_steps
+    # the plain FP64 drop-in, one system after another (natural-order ILU(0), unrestarted)
+    torch.cuda.synchronize()
+    tp = time.time()
+    plain_ok = True
+    for A, B, p in zip(dm, Bd, nrhs):
+        N = bpf.ilu0(A, p)
+        X, s = bpf.block_gmres(A, B, N=N, ldiv=True, restart=False, memory=400, atol=0.0, rtol=RTOL,
+                               itmax=400)
+        plain_ok = plain_ok and s.solved
+    torch.cuda.synchronize()
+    t_plain = time.time() - tp
+    # CPU: the oracle's block-GMRES on a sample of the systems (1 thread), scaled by RHS
+    O.set_threads(1)
+    idx = list(range(0, nsys, max(1, nsys // 8)))[:8]
+    tc = time.time()
+    for k in idx:
+        O.block_gmres(mats[k], Bs[k], N=(1, O.ilu0(mats[k])), memory=400, restart=False, atol=0.0,
+                      rtol=RTOL, itmax=400)
+    t_cpu = time.time() - tc
+    cpu_rhs = sum(nrhs[k] for k in idx)
+    hbm, hbm_src = peaks()
+    achieved = by_b / (ms_b / 1e3) / 1e9 if ms_b > 0 else None
+    tot = {k: int(v.sum()) for k, v in cyc.items()}
+    value = total_rhs * steps / (t_ms / 1e3)
+    line = {"config": {"workload": f"batch{nsys}_grids100-3000_p8-64", "systems": nsys,
+                       "unknowns_total": int(sum(A.shape[0] for A in mats)), "rhs_total": total_rhs,
+                       "nnz_total": int(sum(A.nnz for A in mats)), "units": plan.nunits,
+                       "grid": plan.grid, "slice": tune["slice"], "ctas_per_sm": tune["ctas_per_sm"],
+                       "ordering": "AMD (minimum degree)", "factors": "FP32", "rtol": RTOL,
+                       "l2": "inputs larger than L2 (all systems' bases)"},
+            "metric": "RHS solves/s at 1e-8 residual (batched)", "unit": "RHS solves/s",
+            "value": value, "ms_per_step": t_ms / steps, "steps": steps,
+            "all_solved": solved, "max_relres": worst,
+            "iterations": {"max": int(units["niter"].max()), "mean": float(units["niter"].mean())},
+            "phase_share": {k: round(v / max(tot["total"], 1), 4) for k, v in tot.items() if k != "total"},
+            "gpu_launches": launches,
+            "e2e": {"value": total_rhs / t_e2e, "unit": "RHS solves/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": h2d},
+            "plain_fp64_dropin": {"value": total_rhs / t_plain, "seconds": t_plain, "all_solved": plain_ok,
+                                  "how": "bpf.ilu0 + bpf.block_gmres per system, natural order"},
+            "batched_over_plain": value / (total_rhs / t_plain),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm if achieved else None, "peak_source": hbm_src,
+                         "kernel": "batch graph (factor + persistent solve)",
+                         "bytes_per_step": by_b / max(cnt_b, 1)},
+            "autotune": {"seconds": t_tune, **{k: v for k, v in tune.items() if k != "cached"}},
+            "plan_seconds": t_plan,
+            "cpu_baseline": {"value": cpu_rhs / t_cpu, "unit": "RHS solves/s", "cores": 1, "kind": "port",
+                             "sample": f"{len(idx)} of the {nsys} systems, full solves"},
+            "dtype": "f64 (FP32 factors)", "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernel-only", choices=["trsv", "spmm", "factor", "gram", "gmres", "mlp"], default=None,
@@ -456,12 +584,12 @@ def main():
                     help="iterations the reference arm extrapolates to (the GPU solve's count)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--config", default="headline",
-                    choices=["headline", "gmres300", "bicgstab9k", "rf25k"],
+                    choices=["headline", "gmres300", "bicgstab9k", "rf25k", "batch512"],
                     help="the other benchmark configurations (one JSON line each, one GPU)")
     args = ap.parse_args()
     if args.config != "headline":
         {"gmres300": config_gmres300, "bicgstab9k": config_bicgstab9k,
-         "rf25k": config_rf25k}[args.config](args)
+         "rf25k": config_rf25k, "batch512": config_batch512}[args.config](args)
         return
     if args.kernel_only:
         kernel_only(args.kernel_only, args.reps, args.iters, args.ordering)

@@ -1,11 +1,13 @@
 """BlockPowerFlow-B200: the multi-RHS sparse solve path of exanauts/BlockPowerFlow.jl on B200.
 
 Python mirror of the reference's Julia API (module BlockPowerFlow, src/BlockPowerFlow.jl):
-block_gmres, block_bicgstab, ilu0, ic0, ldiv!, CUSOLVERRF.  Every call runs in libbpf.so
+block_gmres, block_bicgstab, ilu0, ic0, ldiv!, CUSOLVERRF; plus the batched solve of many
+independent systems in one graph launch (BatchPlan).  Every call runs in libbpf.so
 (hand-written sm_100a kernels); there is no CPU fallback.
 """
 from . import cusolverrf as CUSOLVERRF
 from . import grid
+from .batch import BatchPlan, BatchStats, autotune
 from ._lib import (BPFError, DimensionMismatch, SingularException, exported_symbols,
                    kernel_launches)
 from .krylov import BlockGMRESStats, SimpleStats, block_bicgstab, block_gmres
@@ -18,5 +20,5 @@ __all__ = [
     "block_gmres", "block_bicgstab", "BlockGMRESStats", "SimpleStats", "ilu0", "ic0", "ldiv_",
     "ldiv", "NVIDIA_ILU0", "NVIDIA_IC0", "CuSparseMatrixCSR", "mul", "householder", "colmajor",
     "empty_colmajor", "BPFError", "DimensionMismatch", "SingularException", "grid",
-    "exported_symbols", "kernel_launches", "CUSOLVERRF",
+    "exported_symbols", "kernel_launches", "CUSOLVERRF", "BatchPlan", "BatchStats", "autotune",
 ]

@@ -60,6 +60,12 @@ class BicgstabOpts(C.Structure):
                 ("timemax", C.c_double), ("verbose", C.c_int), ("history", C.c_int)]
 
 
+class BatchOpts(C.Structure):
+    _fields_ = [("atol", C.c_double), ("rtol", C.c_double), ("itmax", C.c_int), ("memory", C.c_int),
+                ("factor_dtype", C.c_int), ("ordering", C.c_int), ("slice", C.c_int),
+                ("ctas_per_sm", C.c_int)]
+
+
 class Stats(C.Structure):
     _fields_ = [("niter", C.c_int), ("solved", C.c_int), ("status", C.c_int), ("timer", C.c_double),
                 ("n_residuals", C.c_int), ("residuals_capacity", C.c_int),
@@ -117,6 +123,13 @@ SIGNATURES = {
     "bpf_rf_solve": (_I, [_P, _I, _P, _I]),
     "bpf_rf_info": (_I, [_P, C.POINTER(_I), C.POINTER(_I), _P, _P]),
     "bpf_rf_destroy": (_I, [_P]),
+    "bpf_batch_opts_default": (None, [C.POINTER(BatchOpts)]),
+    "bpf_batch_plan": (_I, [_P, _I, _P, _P, C.POINTER(BatchOpts), C.POINTER(_P)]),
+    "bpf_batch_solve": (_I, [_P, _P, _P, _P, _P, _P]),
+    "bpf_batch_unit_stats": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "bpf_batch_unit_cycles": (_I, [_P, _P]),
+    "bpf_batch_info": (_I, [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(C.c_longlong)]),
+    "bpf_batch_destroy": (_I, [_P]),
 }
 
 _lib = None
@@ -194,7 +207,7 @@ def kernel_launches(device=None) -> int:
 
 
 KERNEL_CLASSES = {"spmm": 0, "trsv": 1, "factor": 2, "gram": 3, "tsmm": 4, "small": 5,
-                  "chol": 6, "hess": 7, "backsub": 8, "mlp": 9}
+                  "chol": 6, "hess": 7, "backsub": 8, "mlp": 9, "batch": 10}
 
 
 def set_timing(on: bool, device=None) -> None:

@@ -421,26 +421,8 @@ static bpf_status prec_create(bpf_ctx *ctx, const bpf_csr_desc *A, int nrhs, int
         std::vector<int> arp, aci;
         BPF_TRY(csr_pattern_to_host(ctx, A, arp, aci, false, nullptr));
         perm = ordering == BPF_ORDER_RCM ? order_rcm(n, arp, aci) : order_min_degree(n, arp, aci);
-        std::vector<int> pinv(n);
-        for (int i = 0; i < n; i++) pinv[perm[i]] = i;
-        rp.assign(n + 1, 0);
-        for (int i = 0; i < n; i++) rp[i + 1] = rp[i] + (arp[perm[i] + 1] - arp[perm[i]]);
-        ci.resize(nnz);
-        amap.resize(nnz);
-        diag.assign(n, -1);
-        std::vector<std::pair<int, int>> row;
-        for (int i = 0; i < n; i++) {
-            const int r = perm[i];
-            row.clear();
-            for (int k = arp[r]; k < arp[r + 1]; k++) row.push_back({pinv[aci[k]], k});
-            std::sort(row.begin(), row.end());
-            for (size_t t = 0; t < row.size(); t++) {
-                ci[rp[i] + t] = row[t].first;
-                amap[row[t].second] = rp[i] + (int)t;
-                if (row[t].first == i) diag[i] = rp[i] + (int)t;
-            }
-            if (diag[i] < 0) return set_error(ctx, BPF_ERR_SINGULAR, "structurally zero diagonal at row %d", r);
-        }
+        const int bad = permute_pattern(n, arp, aci, perm, rp, ci, amap, diag);
+        if (bad >= 0) return set_error(ctx, BPF_ERR_SINGULAR, "structurally zero diagonal at row %d", bad);
     }
     bpf_prec *P = nullptr;
     BPF_TRY(prec_setup(ctx, kind, n, rp, ci, diag, &P));

@@ -122,4 +122,31 @@ std::vector<int> order_rcm(int n, const std::vector<int> &rp, const std::vector<
     return order;
 }
 
+int permute_pattern(int n, const std::vector<int> &arp, const std::vector<int> &aci,
+                    const std::vector<int> &perm, std::vector<int> &rp, std::vector<int> &ci,
+                    std::vector<int> &amap, std::vector<int> &diag) {
+    const int nnz = arp[n];
+    std::vector<int> pinv(n);
+    for (int i = 0; i < n; i++) pinv[perm[i]] = i;
+    rp.assign(n + 1, 0);
+    for (int i = 0; i < n; i++) rp[i + 1] = rp[i] + (arp[perm[i] + 1] - arp[perm[i]]);
+    ci.resize(nnz);
+    amap.resize(nnz);
+    diag.assign(n, -1);
+    std::vector<std::pair<int, int>> row;
+    for (int i = 0; i < n; i++) {
+        const int r = perm[i];
+        row.clear();
+        for (int k = arp[r]; k < arp[r + 1]; k++) row.push_back({pinv[aci[k]], k});
+        std::sort(row.begin(), row.end());
+        for (size_t t = 0; t < row.size(); t++) {
+            ci[rp[i] + t] = row[t].first;
+            amap[row[t].second] = rp[i] + (int)t;
+            if (row[t].first == i) diag[i] = rp[i] + (int)t;
+        }
+        if (diag[i] < 0) return r;
+    }
+    return -1;
+}
+
 }  // namespace bpf

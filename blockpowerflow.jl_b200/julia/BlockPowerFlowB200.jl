@@ -13,7 +13,7 @@ using CUDA.CUSPARSE
 
 import LinearAlgebra: ldiv!
 
-export block_gmres, block_bicgstab, ilu0, ic0, CUSOLVERRF
+export block_gmres, block_bicgstab, ilu0, ic0, CUSOLVERRF, BatchPlan, batch_solve!
 
 const libbpf = joinpath(@__DIR__, "..", "lib", "libbpf.so")
 
@@ -193,6 +193,52 @@ function block_gmres(A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64},
                                      history ? res[1:min(s.n_residuals, cap)] : Float64[],
                                      s.timer, status_string(s.status))
     return X, stats
+end
+
+# ---- batched block-GMRES (an addition: many systems in one graph launch) ----------------
+struct BatchOpts
+    atol::Cdouble
+    rtol::Cdouble
+    itmax::Cint
+    memory::Cint
+    factor_dtype::Cint
+    ordering::Cint
+    slice::Cint
+    ctas_per_sm::Cint
+end
+
+mutable struct BatchPlan
+    h::Ptr{Cvoid}
+    mats::Vector{CuSparseMatrixCSR{Float64,Cint}}   # kept alive: their values are re-read per solve
+    nrhs::Vector{Int}
+end
+
+function BatchPlan(As::Vector{CuSparseMatrixCSR{Float64,Cint}}, nrhs::Vector{Int}; atol=0.0, rtol=1e-8,
+                   itmax=0, memory=0, factor_type=Float32, ordering=:AMD, slice=0, ctas_per_sm=0)
+    length(As) == length(nrhs) || throw(DimensionMismatch("one nrhs per system expected"))
+    descs = [desc(A) for A in As]
+    opts = Ref(BatchOpts(atol, rtol, itmax, memory, factor_type === Float32 ? 1 : 0,
+                         PREC_ORDER[ordering], slice, ctas_per_sm))
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:bpf_batch_plan, libbpf), Cint,
+                (Ptr{Cvoid}, Cint, Ptr{CsrDesc}, Ptr{Cint}, Ref{BatchOpts}, Ref{Ptr{Cvoid}}),
+                ctx(), length(As), descs, Cint.(nrhs), opts, r))
+    P = BatchPlan(r[], As, nrhs)
+    finalizer(p -> ccall((:bpf_batch_destroy, libbpf), Cint, (Ptr{Cvoid},), p.h), P)
+    return P
+end
+
+# Xs[s] = As[s] \ Bs[s] for every system; returns per-system (niter, solved, status).
+function batch_solve!(Xs::Vector{CuMatrix{Float64}}, P::BatchPlan, Bs::Vector{CuMatrix{Float64}})
+    ns = length(P.nrhs)
+    length(Bs) == ns == length(Xs) || throw(DimensionMismatch("one block per system expected"))
+    buf = Vector{UInt8}(undef, ns * sizeof(CStats))
+    check(ccall((:bpf_batch_solve, libbpf), Cint,
+                (Ptr{Cvoid}, Ptr{CuPtr{Cdouble}}, Ptr{Cint}, Ptr{CuPtr{Cdouble}}, Ptr{Cint}, Ptr{UInt8}),
+                P.h, [pointer(B) for B in Bs], Cint[stride(B, 2) for B in Bs],
+                [pointer(X) for X in Xs], Cint[stride(X, 2) for X in Xs], buf))
+    stats = [unsafe_load(Ptr{CStats}(pointer(buf)) + (s - 1) * sizeof(CStats)) for s in 1:ns]
+    return [(niter=Int(c.niter), solved=c.solved != 0, status=status_string(c.status)) for c in stats]
 end
 
 # ---- block-BiCGSTAB (src/block_bicgstab.jl:182-299) -----------------------------------

@@ -142,7 +142,8 @@ typedef enum {
     BPF_KC_HESS = 7,    /* block Hessenberg QR update (apply + factor) */
     BPF_KC_BACKSUB = 8, /* block back substitution of block-GMRES     */
     BPF_KC_MLP = 9,     /* learned warm start: tensor-core GEMMs       */
-    BPF_KC_COUNT = 10
+    BPF_KC_BATCH = 10,  /* batched solve: factor + persistent solve graph */
+    BPF_KC_COUNT = 11
 } bpf_kernel_class;
 BPF_API bpf_status bpf_ctx_set_timing(bpf_ctx *ctx, int on);
 /* Totals since bpf_ctx_set_timing(ctx, 1): device milliseconds, launches, and the launches'
@@ -286,6 +287,50 @@ BPF_API bpf_status bpf_block_bicgstab(bpf_ctx *ctx, const bpf_csr_desc *A, int p
                                       const double *B, int ldb, double *X, int ldx,
                                       const double *C, int ldc, const bpf_prec *N,
                                       const bpf_bicgstab_opts *opts, bpf_stats *stats);
+
+/* ---- batched block-GMRES ----------------------------------------------------------------
+ * Many independent systems, each with its own Jacobian and right-hand-side block, solved by
+ * ILU(0)-preconditioned block-GMRES in one CUDA-graph launch: the ILU(0) of every system, then
+ * ONE persistent kernel in which each CTA takes work units (a system and a slice of <= 32 of its
+ * right-hand-side columns) from a queue, longest first.  No counterpart in the reference, whose
+ * solvers take one system per call; each unit follows block_gmres (src/block_gmres.jl:170-411)
+ * with a right ILU(0) (src/preconditioners_nvidia.jl:42-71), unrestarted while its basis lasts.
+ * Stopping test per unit: ||R_slice||_F <= atol + rtol ||B_slice||_F (so the whole block meets
+ * ||R||_F <= rtol ||B||_F when atol = 0). */
+typedef struct bpf_batch bpf_batch;
+typedef struct {
+    double atol;        /* default 0 */
+    double rtol;        /* default 1e-8 */
+    int itmax;          /* iterations per unit; 0 -> 2 * div(n, q) */
+    int memory;         /* basis blocks per unit; 0 -> sized from n and q (restart when full) */
+    int factor_dtype;   /* BPF_F32 (default: FP32 factors, flexible FP64 outer) or BPF_F64 */
+    int ordering;       /* BPF_ORDER_AMD (default, minimum degree), _MDQ, _RCM or _NATURAL */
+    int slice;          /* widest column slice q, 1..32; 0 -> 16 */
+    int ctas_per_sm;    /* resident solve CTAs per SM, 1 or 2; 0 -> 2 */
+} bpf_batch_opts;
+BPF_API void bpf_batch_opts_default(bpf_batch_opts *opts);
+/* Analyse nsys systems (A[s]: device CSR, FP64; nrhs[s] >= 1 columns) and capture the solve
+ * graph.  A[s].vals is re-read by every solve: new values on the same pattern go in place. */
+BPF_API bpf_status bpf_batch_plan(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A, const int *nrhs,
+                                  const bpf_batch_opts *opts, bpf_batch **batch);
+/* X[s] (n_s x nrhs[s], column-major, ld ldx[s]) = A[s] \ B[s] for every s; B, X, ldb, ldx are
+ * HOST arrays of nsys entries (device block pointers; ldb / ldx NULL -> n_s).  stats (nsys
+ * entries, nullable): niter = the most iterations of the system's units, solved = all units
+ * met the tolerance, npass = most restart cycles.  BPF_ERR_SINGULAR names the first system whose
+ * ILU(0) met a zero pivot (the other systems are still solved). */
+BPF_API bpf_status bpf_batch_solve(bpf_batch *batch, const double *const *B, const int *ldb,
+                                   double *const *X, const int *ldx, bpf_stats *stats);
+/* Per unit of the last solve (arrays of bpf_batch_info's nunits entries, each nullable). */
+BPF_API bpf_status bpf_batch_unit_stats(const bpf_batch *batch, int *sys, int *col0, int *q,
+                                        int *memory, int *niter, int *status, double *rnorm0,
+                                        double *rnorm);
+/* SM cycles of each unit of the last solve by phase: 8 entries per unit (triangular solves,
+ * SpMM, Gram products, block updates, Cholesky-QR, Hessenberg update, back substitution, and
+ * the unit's total), counted by thread 0 of the unit's CTA. */
+BPF_API bpf_status bpf_batch_unit_cycles(const bpf_batch *batch, long long *cycles);
+BPF_API bpf_status bpf_batch_info(const bpf_batch *batch, int *nunits, int *grid,
+                                  long long *device_bytes);
+BPF_API bpf_status bpf_batch_destroy(bpf_batch *batch);
 
 /* ---- refactorization (cusolverRF replacement) ------------------------------------------ */
 /* CusolverRfLU(A; ordering, tol, fast_mode) / CusolverRfLUBatch(A, batch; ...):
