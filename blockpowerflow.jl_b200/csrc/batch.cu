@@ -170,7 +170,7 @@ __device__ double cta_sum(double v, double *scratch) {
 template <int NT>
 __device__ void gram_t(const double *A, const double *B, int n, int q, double *red, double *dst, int ldd) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-    constexpr int UF = NT == 1 ? 8 : (NT == 2 ? 4 : 2);
+    constexpr int UF = NT == 1 ? 16 : (NT == 2 ? 8 : (NT == 3 ? 4 : 2));
     double acc[NT][NT][2];
 #pragma unroll
     for (int a = 0; a < NT; a++)
@@ -231,16 +231,18 @@ __device__ __noinline__ void gram(const double *V, size_t vstr, int nblk, const 
 
 // ---------------------------------------------------------------------------------------
 // W (n x q) = [W] + sign * sum_{i < nb} A_i C_i, A_i = A + i astr (row-major n x q), C_i = C + i
-// cstr (q x q, row stride ldc).  A warp owns 8 MT consecutive rows at a time; W may be A itself
-// (nb = 1, init = false: the warp reads its rows before it writes them).  No barrier inside.
+// cstr (q x q, row stride ldc).  A warp owns 8 MT consecutive rows at a time; for each block i it
+// loads the fragments of all of the block's k-steps (MT + NT per k-step) before their DMMAs, so
+// a block costs one memory latency.  W may be A itself (nb = 1, init = false: the warp reads its
+// rows before it writes them).  No barrier inside.
 // ---------------------------------------------------------------------------------------
 template <int NT>
 __device__ void update_t(double *W, const double *A, size_t astr, const double *C, size_t cstr, int ldc,
                          int nb, int n, int q, double sign, bool init) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-    constexpr int MT = NT == 1 ? 8 : (NT == 2 ? 4 : 2);
+    constexpr int MT = NT == 1 ? 8 : (NT == 2 ? 4 : (NT == 3 ? 2 : 1));
+    constexpr int KK = 2 * NT;   // k-steps of 4 columns in a block of q <= 8 NT columns
     constexpr int RT = 8 * MT;
-    const int kk = (q + 3) >> 2;
     for (int r0 = warp * RT; r0 < n; r0 += kW * RT) {
         double acc[MT][NT][2];
 #pragma unroll
@@ -254,24 +256,27 @@ __device__ void update_t(double *W, const double *A, size_t astr, const double *
         for (int i = 0; i < nb; i++) {
             const double *Ai = A + i * astr;
             const double *Ci = C + i * cstr;
-            for (int k = 0; k < kk; k++) {
+            double bf[KK][NT], af[KK][MT];
+#pragma unroll
+            for (int k = 0; k < KK; k++) {
                 const int kc = k * 4 + t;
-                double bf[NT], af[MT];
 #pragma unroll
                 for (int b = 0; b < NT; b++) {
                     const int c = b * 8 + g;
-                    bf[b] = (kc < q && c < q) ? sign * Ci[kc * ldc + c] : 0.0;
+                    bf[k][b] = (kc < q && c < q) ? Ci[kc * ldc + c] : 0.0;
                 }
 #pragma unroll
                 for (int m = 0; m < MT; m++) {
                     const int r = r0 + m * 8 + g;
-                    af[m] = (kc < q && r < n) ? Ai[(size_t)r * q + kc] : 0.0;
+                    af[k][m] = (kc < q && r < n) ? Ai[(size_t)r * q + kc] : 0.0;
                 }
+            }
+#pragma unroll
+            for (int k = 0; k < KK; k++)
 #pragma unroll
                 for (int m = 0; m < MT; m++)
 #pragma unroll
-                    for (int b = 0; b < NT; b++) dmma(acc[m][b][0], acc[m][b][1], af[m], bf[b]);
-            }
+                    for (int b = 0; b < NT; b++) dmma(acc[m][b][0], acc[m][b][1], sign * af[k][m], bf[k][b]);
         }
 #pragma unroll
         for (int m = 0; m < MT; m++)
