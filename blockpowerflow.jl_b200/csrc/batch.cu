@@ -98,7 +98,7 @@ struct IO {
 
 struct Cfg {
     double atol, rtol;
-    int itmax;      // per unit (0: 2 * floor(n / q))
+    int itmax;      // per unit (0: max(2 floor(n / q), 50))
     int f32;        // FP32 factors
 };
 
@@ -170,12 +170,15 @@ __device__ double cta_sum(double v, double *scratch) {
 template <int NT>
 __device__ void gram_t(const double *A, const double *B, int n, int q, double *red, double *dst, int ldd) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-    constexpr int UF = NT == 1 ? 16 : (NT == 2 ? 8 : (NT == 3 ? 4 : 2));
-    double acc[NT][NT][2];
+    constexpr int UF = NT == 1 ? 16 : (NT == 2 ? 8 : 2);
+    constexpr int NC = NT <= 3 ? 2 : 1;   // independent accumulator chains (alternate k-steps)
+    double acc[NC][NT][NT][2];
 #pragma unroll
-    for (int a = 0; a < NT; a++)
+    for (int h = 0; h < NC; h++)
 #pragma unroll
-        for (int b = 0; b < NT; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
+        for (int a = 0; a < NT; a++)
+#pragma unroll
+            for (int b = 0; b < NT; b++) acc[h][a][b][0] = acc[h][a][b][1] = 0.0;
     const int nks = (n + 3) >> 2;
     for (int ks0 = warp * UF; ks0 < nks; ks0 += kW * UF) {
         double af[UF][NT], bf[UF][NT];
@@ -195,15 +198,22 @@ __device__ void gram_t(const double *A, const double *B, int n, int q, double *r
 #pragma unroll
             for (int a = 0; a < NT; a++)
 #pragma unroll
-                for (int b = 0; b < NT; b++) dmma(acc[a][b][0], acc[a][b][1], af[u][a], bf[u][b]);
+                for (int b = 0; b < NT; b++)
+                    dmma(acc[u % NC][a][b][0], acc[u % NC][a][b][1], af[u][a], bf[u][b]);
     }
     double *my = red + warp * kLd * kLd;
 #pragma unroll
     for (int a = 0; a < NT; a++)
 #pragma unroll
         for (int b = 0; b < NT; b++) {
-            my[(a * 8 + g) * kLd + b * 8 + 2 * t] = acc[a][b][0];
-            my[(a * 8 + g) * kLd + b * 8 + 2 * t + 1] = acc[a][b][1];
+            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+            for (int h = 0; h < NC; h++) {
+                s0 += acc[h][a][b][0];
+                s1 += acc[h][a][b][1];
+            }
+            my[(a * 8 + g) * kLd + b * 8 + 2 * t] = s0;
+            my[(a * 8 + g) * kLd + b * 8 + 2 * t + 1] = s1;
         }
     __syncthreads();
     for (int idx = threadIdx.x; idx < q * q; idx += kT) {
@@ -757,7 +767,7 @@ __device__ void solve_unit(const Sys &S, const Unit &U, const IO &io, const Cfg 
     }
     const double rn0 = sqrt(cta_sum(s, sm.scal));
     const double eps = cfg.atol + cfg.rtol * rn0;
-    const int itmax = cfg.itmax > 0 ? cfg.itmax : max(2 * (n / q), 1);
+    const int itmax = cfg.itmax > 0 ? cfg.itmax : max(2 * (n / q), 50);
     int iter = 0, cycles = 0, status = BPF_SOLVE_UNKNOWN;
     double rn = rn0;
     bool solved = rn0 <= eps;
@@ -859,14 +869,26 @@ __device__ void solve_unit(const Sys &S, const Unit &U, const IO &io, const Cfg 
             __syncthreads();
             pc.mark(PH_UPDATE);
         }
-        if (solved || iter >= itmax) break;
         if (brk && j == 0) {
             status = -1;
             break;
         }
-        // restart from the true residual
+        // the true residual: the next cycle's start, and the check of a converged estimate (the
+        // least-squares residual can fall below eps while B - A X has not, when rounding has
+        // eroded the basis' orthogonality); a failed check refines from the true residual
         spmm(S, q, U.Xh, U.V, U.Bh);
         __syncthreads();
+        if (solved) {
+            double s2 = 0.0;
+            for (size_t idx = threadIdx.x; idx < bs; idx += kT) {
+                const double v = U.V[idx];
+                s2 += v * v;
+            }
+            rn = sqrt(cta_sum(s2, sm.scal));
+            if (rn <= eps) break;
+            solved = false;
+        }
+        pc.mark(PH_SPMM);
     }
     if (status != -1) status = solved ? BPF_SOLVE_SOLVED : BPF_SOLVE_ITMAX;
     __syncthreads();
@@ -1183,9 +1205,12 @@ bpf_status bpf_batch_plan(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A, const i
         b->n[s] = n;
         b->p[s] = nrhs[s];
         vals[s] = D.vals;
-        // work units: ceil(p / qmax) slices of nearly equal width
+        // work units: ceil(p / q_s) slices of nearly equal width, q_s = min(qmax, n / 24): a block
+        // wider than n / 24 exhausts the Krylov space of a small system within a few iterations,
+        // where a partial breakdown (directions that have converged) stalls block-GMRES
         const int p = nrhs[s];
-        const int ns = (p + qmax - 1) / qmax;
+        const int qs = std::max(1, std::min(qmax, n / 24));
+        const int ns = (p + qs - 1) / qs;
         int col = 0;
         for (int k = 0; k < ns; k++) {
             const int q = p / ns + (k < p % ns ? 1 : 0);
@@ -1195,7 +1220,7 @@ bpf_status bpf_batch_plan(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A, const i
             un.q = q;
             un.m = o.memory > 0 ? o.memory : auto_memory(n, q);
             if (o.itmax > 0) un.m = std::min(un.m, o.itmax);
-            un.m = std::max(1, std::min(un.m, n / q + 2));   // the Krylov space has at most n columns
+            un.m = std::max(1, std::min(un.m, n / q - 1));   // (m + 1) q <= n: the basis stays in R^n
             // cost: basis traffic ~ iterations^2 n q plus per-iteration level latency
             const double it = std::min((double)un.m, 1.5 * pow((double)n / q, 0.7));
             un.est = it * it * (double)n * q * 8.0 + it * (L.nlev + U.nlev) * 2.0e4;

@@ -301,7 +301,7 @@ typedef struct bpf_batch bpf_batch;
 typedef struct {
     double atol;        /* default 0 */
     double rtol;        /* default 1e-8 */
-    int itmax;          /* iterations per unit; 0 -> 2 * div(n, q) */
+    int itmax;          /* iterations per unit; 0 -> max(2 div(n, q), 50) */
     int memory;         /* basis blocks per unit; 0 -> sized from n and q (restart when full) */
     int factor_dtype;   /* BPF_F32 (default: FP32 factors, flexible FP64 outer) or BPF_F64 */
     int ordering;       /* BPF_ORDER_AMD (default, minimum degree), _MDQ, _RCM or _NATURAL */
