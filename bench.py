@@ -551,6 +551,10 @@ def config_batch512(args):
             "all_solved": solved, "max_relres": worst,
             "iterations": {"max": int(units["niter"].max()), "mean": float(units["niter"].mean())},
             "phase_share": {k: round(v / max(tot["total"], 1), 4) for k, v in tot.items() if k != "total"},
+            "unit_cycles": {"max": int(cyc["total"].max()), "mean": float(cyc["total"].mean()),
+                            "sum": int(cyc["total"].sum()),
+                            "balanced_bound_ms": float(cyc["total"].sum()) / plan.grid / 1.965e6,
+                            "critical_path_ms": float(cyc["total"].max()) / 1.965e6},
             "gpu_launches": launches,
             "e2e": {"value": total_rhs / t_e2e, "unit": "RHS solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": h2d},

@@ -34,6 +34,17 @@ __device__ __forceinline__ bool gate_off(const SolveState *st, const int *gate,
     return false;
 }
 
+// The gate decided once per CTA (thread 0 reads it): st->active is cleared by the Hessenberg
+// update on the other stream, possibly between the reads of two warps, and warps that disagreed
+// would leave some of the CTA past a barrier the others never reach.
+__device__ __forceinline__ bool cta_gate_off(const SolveState *st, const int *gate, const int *gate2 = nullptr) {
+    __shared__ int s_off;
+    if (threadIdx.x == 0) s_off = gate_off(st, gate, gate2) ? 1 : 0;
+    __syncthreads();
+    return s_off != 0;
+}
+
+
 // ---------------------------------------------------------------------------------------
 // gram
 // ---------------------------------------------------------------------------------------
@@ -43,7 +54,7 @@ gram_partial_kernel(int n, int p, int nb, const double *__restrict__ A, size_t s
                     const double *__restrict__ B, double *__restrict__ partial,
                     int rows_per_chunk, const SolveState *st, const int *gate,
                     const int *gate2) {
-    if (gate_off(st, gate, gate2)) return;
+    if (cta_gate_off(st, gate, gate2)) return;
     constexpr int TPD = GT / 16;   // outputs per thread per dimension
     __shared__ double As[kGramRows][GT];
     __shared__ double Bs[kGramRows][GT];
@@ -98,7 +109,7 @@ __global__ void gram_reduce_kernel(int total, int nchunks, const double *__restr
                                    double *__restrict__ out, double alpha, int accumulate,
                                    double *__restrict__ out2, const SolveState *st,
                                    const int *gate, const int *gate2) {
-    if (gate_off(st, gate, gate2)) return;
+    if (cta_gate_off(st, gate, gate2)) return;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
         double s = 0.0;
         for (int c = 0; c < nchunks; c++) s += partial[(size_t)c * total + e];
@@ -248,7 +259,7 @@ __global__ void __launch_bounds__(128)
 gram_dmma_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
                  const double *__restrict__ B, double *__restrict__ partial, int rows_per_chunk,
                  const SolveState *st, const int *gate, const int *gate2) {
-    if (gate_off(st, gate, gate2)) return;
+    if (cta_gate_off(st, gate, gate2)) return;
     constexpr int RS = 32, S = GT + 4, WT = GT / 2, MT = WT / 8;
     __shared__ double As[RS * S];
     __shared__ double Bs[RS * S];
@@ -307,15 +318,18 @@ gram_dmma_kernel(int n, int p, int nb, const double *__restrict__ A, size_t stri
 // Same product with the row chunks grouped in clusters of 8 CTAs: the 8 partial tiles are
 // summed through distributed shared memory (each CTA of the cluster sums 1/8 of the tile's
 // rows over the 8 CTAs) and one partial per cluster goes to global memory, an 8x cut of the
-// partial-sum traffic.  The gate is uniform across a cluster, so either every CTA of a
-// cluster returns early or none does.
+// partial-sum traffic.  A gated-off CTA does not return early: its peers read its shared memory
+// in the cluster sum, and the gate (st->active, cleared by the Hessenberg update on the other
+// stream) may read differently in two CTAs of one cluster; it runs no row stages and stores
+// nothing (such a launch belongs to an iteration past the stopping point, whose results are
+// discarded).
 template <int GT>
 __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(128)
 gram_dmma_cl_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
                     const double *__restrict__ B, double *__restrict__ partial,
                     int rows_per_chunk, const SolveState *st, const int *gate,
                     const int *gate2) {
-    if (gate_off(st, gate, gate2)) return;
+    const bool off = cta_gate_off(st, gate, gate2);
     namespace cg = cooperative_groups;
     constexpr int RS = 32, S = GT + 4, WT = GT / 2, MT = WT / 8;
     __shared__ double sbuf[2 * RS * S];
@@ -324,7 +338,7 @@ gram_dmma_cl_kernel(int n, int p, int nb, const double *__restrict__ A, size_t s
     const int ntile = (p + GT - 1) / GT;
     const int a0 = (blockIdx.z / ntile) * GT, b0 = (blockIdx.z % ntile) * GT;
     const int r_begin = chunk * rows_per_chunk;
-    const int r_end = min(n, r_begin + rows_per_chunk);
+    const int r_end = off ? r_begin : min(n, r_begin + rows_per_chunk);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t4 = lane & 3;
     const double *Aj = A + (size_t)j * strideA;
@@ -374,7 +388,7 @@ gram_dmma_cl_kernel(int n, int p, int nb, const double *__restrict__ A, size_t s
         double s = 0.0;
 #pragma unroll
         for (int q = 0; q < 8; q++) s += cluster.map_shared_rank(sbuf, q)[a * GT + b];
-        if (a0 + a < p && b0 + b < p) out[(size_t)(a0 + a) * p + b0 + b] = s;
+        if (!off && a0 + a < p && b0 + b < p) out[(size_t)(a0 + a) * p + b0 + b] = s;
     }
     cluster.sync();
 }
@@ -386,7 +400,7 @@ tsmm_dmma_kernel(int n, int p, int nb, const double *__restrict__ A, size_t stri
                  const double *__restrict__ S, size_t strideS, double alpha, const double *Cin,
                  double beta, double *Out, const SolveState *st, const int *nb_dev,
                  const int *gate, const int *gate2) {
-    if (gate_off(st, gate, gate2)) return;
+    if (cta_gate_off(st, gate, gate2)) return;
     constexpr int KC = 32, SA = KC + 4, SB = GT + 4, WN = GT / 2, MTN = WN / 8;
     __shared__ double As[64 * SA];
     __shared__ double Bs[KC * SB];
@@ -473,7 +487,7 @@ __global__ void __launch_bounds__(256, 2)
 tsmm_pipe_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
                  const double *__restrict__ S, size_t strideS, double alpha, const double *Cin,
                  double beta, double *Out, const SolveState *st, const int *gate, const int *gate2) {
-    if (gate_off(st, gate, gate2)) return;
+    if (cta_gate_off(st, gate, gate2)) return;
     constexpr int BM = 64, GT = 64, KC = 32, SA = KC + 4, SB = GT + 4, ST = kPipeStages;
     extern __shared__ __align__(16) double psm[];
     double *As = psm;                          // ST x BM x SA
@@ -559,12 +573,13 @@ tsmm_pipe_kernel(int n, int p, int nb, const double *__restrict__ A, size_t stri
 
 // Partial Gram tile (a0.., b0..) of A_j^T B over one chunk of rows; chunks grouped in clusters
 // of 8 CTAs whose partial tiles are summed through distributed shared memory (one partial per
-// cluster goes to global memory).  The gate is uniform across a cluster.
+// cluster goes to global memory).  A gated-off CTA runs no row stages and stores nothing but
+// stays for the cluster sum (see gram_dmma_cl_kernel).
 __global__ void __launch_bounds__(256)
 gram_pipe_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
                  const double *__restrict__ B, double *__restrict__ partial, int rows_per_chunk,
                  const SolveState *st, const int *gate, const int *gate2, GramEpilogue ep) {
-    if (gate_off(st, gate, gate2)) return;
+    const bool off = cta_gate_off(st, gate, gate2);
     namespace cg = cooperative_groups;
     constexpr int GT = 64, RS = 32, SB = GT + 4, ST = kPipeStages;
     extern __shared__ __align__(16) double psm[];
@@ -574,7 +589,7 @@ gram_pipe_kernel(int n, int p, int nb, const double *__restrict__ A, size_t stri
     const int ntile = (p + GT - 1) / GT;
     const int a0 = (blockIdx.z / ntile) * GT, b0 = (blockIdx.z % ntile) * GT;
     const int r_begin = chunk * rows_per_chunk;
-    const int r_end = min(n, r_begin + rows_per_chunk);
+    const int r_end = off ? r_begin : min(n, r_begin + rows_per_chunk);
     const int nst = r_end > r_begin ? (r_end - r_begin + RS - 1) / RS : 0;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t4 = lane & 3;
@@ -648,7 +663,7 @@ gram_pipe_kernel(int n, int p, int nb, const double *__restrict__ A, size_t stri
         const int a = rank * rpr + e / GT, b = e % GT;
         double sum = 0.0;
         for (int q = 0; q < cs; q++) sum += cluster.map_shared_rank(tile, q)[a * GT + b];
-        if (a0 + a < p && b0 + b < p) {
+        if (!off && a0 + a < p && b0 + b < p) {
             const size_t idx = (size_t)(a0 + a) * p + b0 + b;
             if (ep.direct) {   // one cluster per block: the final result, as the reduce kernel
                 double v = ep.alpha * sum;
@@ -684,7 +699,7 @@ tsmm_kernel(int n, int p, int nb, const double *__restrict__ A, size_t strideA,
             const double *__restrict__ S, size_t strideS, double alpha, const double *Cin,
             double beta, double *Out, const SolveState *st, const int *nb_dev, const int *gate,
             const int *gate2) {
-    if (gate_off(st, gate, gate2)) return;
+    if (cta_gate_off(st, gate, gate2)) return;
     constexpr int TPD = GT / 16;
     constexpr int RPT = kTsmmRows / 16;
     __shared__ double As[kTsmmRows][kTsmmK + 1];
@@ -784,7 +799,7 @@ bpf_status tsmm(bpf_ctx *ctx, int n, int p, int nb, const double *A, size_t stri
 __global__ void gated_copy_kernel(size_t len, const double *__restrict__ src,
                                   double *__restrict__ dst, const SolveState *st, const int *gate,
                                   const int *gate2) {
-    if (gate_off(st, gate, gate2)) return;
+    if (cta_gate_off(st, gate, gate2)) return;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < len;
          e += (size_t)gridDim.x * blockDim.x)
         dst[e] = src[e];
@@ -825,7 +840,7 @@ __global__ void reorth_fold_kernel(int p, int nb, double *__restrict__ Psi,
                                    const double *__restrict__ C2, double *__restrict__ C,
                                    double *__restrict__ scratch, const SolveState *st,
                                    const int *gate) {
-    if (gate_off(st, gate)) return;
+    if (cta_gate_off(st, gate)) return;
     const size_t pp = (size_t)p * p;
     const size_t total = (size_t)nb * pp;
     // blocks 0..nb-1: Psi update; block nb (one extra p x p) : C2 R1 into scratch
@@ -867,7 +882,7 @@ bpf_status reorth_fold(bpf_ctx *ctx, int p, int nb, double *Psi, const double *P
 // ---------------------------------------------------------------------------------------
 __global__ void axpby_kernel(size_t len, double a, const double *__restrict__ x, double b,
                              double *__restrict__ y, const SolveState *st) {
-    if (st && !st->active) return;
+    if (cta_gate_off(st, nullptr)) return;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < len;
          e += (size_t)gridDim.x * blockDim.x)
         y[e] = a * x[e] + (b == 0.0 ? 0.0 : b * y[e]);

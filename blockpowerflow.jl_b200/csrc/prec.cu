@@ -481,11 +481,22 @@ template <int G, int CPL, typename TF, bool IN_F32, bool OUT_F32>
 __global__ void __launch_bounds__(512)
 trsv2_coop_kernel(TriKernelArgs t0, TriKernelArgs t1, int p, const void *Xv, void *Yv,
                   DevStatus *ds, const int *gate, const int *perm, double *Zv) {
-    if (gate && *gate == 0) return;
     __shared__ unsigned s_gen;
+    __shared__ int s_skip;
     if (threadIdx.x == 0) s_gen = barrier_gen_start(ds);
     __syncthreads();
     unsigned gen = s_gen;
+    if (gate) {
+        // The gate (st->active) may be cleared by the other stream while the CTAs start, so CTAs
+        // reading it themselves could disagree and leave the others waiting at a level barrier.
+        // One decision for the grid: CTA 0 snapshots the gate before a barrier, every CTA reads
+        // the snapshot after it, and either all CTAs leave or none does.
+        if (blockIdx.x == 0 && threadIdx.x == 0) ds->pad[0] = (*gate == 0) ? 1 : 0;
+        if (!grid_barrier(ds, gen)) return;
+        if (threadIdx.x == 0) s_skip = ld_relaxed_i32(&ds->pad[0]);
+        __syncthreads();
+        if (s_skip) return;
+    }
     using TIn = typename std::conditional<IN_F32, float, double>::type;
     using TOut = typename std::conditional<OUT_F32, float, double>::type;
     const TIn *X = (const TIn *)Xv;

@@ -169,9 +169,13 @@ chol3_kernel(int n, int p, const double *__restrict__ G, double *__restrict__ Ri
              double *__restrict__ Racc, double *__restrict__ gscr, int pass, SolveState *st,
              const int *gate, const int *gate2, int *shift_flag, int *reorth_flag,
              DevStatus *ds, int iter_tag) {
-    if (st && !st->active) return;
-    if (gate && *gate == 0) return;
-    if (gate2 && *gate2 == 0) return;
+    {   // one decision per CTA: st->active may be cleared by the other stream mid-launch
+        __shared__ int s_off;
+        if (threadIdx.x == 0)
+            s_off = ((st && !st->active) || (gate && *gate == 0) || (gate2 && *gate2 == 0)) ? 1 : 0;
+        __syncthreads();
+        if (s_off) return;
+    }
     extern __shared__ __align__(128) double sm[];
     const int ld = p + 1;
     double *g = sm;                                   // p x ld

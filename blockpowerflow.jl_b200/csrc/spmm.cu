@@ -19,7 +19,11 @@ spmm_rm_kernel(int n, const int *__restrict__ rp, const int *__restrict__ ci,
                const double *__restrict__ av, int base, int p, double alpha,
                const TX *__restrict__ X, double beta, double *__restrict__ Y,
                const double *__restrict__ Bres, const int *gate) {
-    if (gate && *gate == 0) return;
+    // one decision per CTA: the gate (st->active) may be cleared by the other stream mid-launch
+    __shared__ int s_off;
+    if (threadIdx.x == 0) s_off = (gate && *gate == 0) ? 1 : 0;
+    __syncthreads();
+    if (s_off) return;
     const int lane = threadIdx.x & 31;
     const int glane = lane % G;                    // lane within the row group
     const int groups_per_block = blockDim.x / G;
