@@ -317,7 +317,8 @@ BPF_API bpf_status bpf_batch_plan(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A,
  * HOST arrays of nsys entries (device block pointers; ldb / ldx NULL -> n_s).  stats (nsys
  * entries, nullable): niter = the most iterations of the system's units, solved = all units
  * met the tolerance, npass = most restart cycles.  BPF_ERR_SINGULAR names the first system whose
- * ILU(0) met a zero pivot (the other systems are still solved). */
+ * ILU(0) met a zero pivot (the other systems are still solved).  Synchronizes the context's
+ * stream; one solve of a plan at a time (its unit workspaces and IO table are shared). */
 BPF_API bpf_status bpf_batch_solve(bpf_batch *batch, const double *const *B, const int *ldb,
                                    double *const *X, const int *ldx, bpf_stats *stats);
 /* Per unit of the last solve (arrays of bpf_batch_info's nunits entries, each nullable). */
