@@ -441,6 +441,62 @@ def config_bicgstab9k(args):
     print(json.dumps(line), flush=True)
 
 
+def config_newton9k(args):
+    """The caller of the solve path: Newton power flow on the 9,000-bus grid (16,998 unknowns)
+    from an operating point perturbed by N(0, 0.001) (from N(0, 0.01) Newton stalls on this random
+    operating point), every step a refactorization + solve on the
+    device (cusolverRF-style path), then the sensitivities dx/du = -Gx^{-1} Gu to the 1,001
+    control voltages (slack and PV) as one multi-RHS solve.  Beside it: the same loop with SciPy's
+    SuperLU (1 core)."""
+    import numpy as np
+    import torch
+
+    import blockpowerflow_b200 as bpf
+    from blockpowerflow_b200 import grid as g
+    from blockpowerflow_b200 import newton as NT
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+
+    prob = NT.make_problem(g.make_grid(N_BUS, N_PV, seed=0))
+    x0 = NT.perturbed_start(prob, 0.001, seed=1)
+    NT.newton(prob, solver="rf", x0=x0, tol=1e-10, sensitivities=True)   # warm-up (analysis, JIT)
+    torch.cuda.synchronize()
+    bpf._lib.set_timing(True)
+    t0 = time.time()
+    r = NT.newton(prob, solver="rf", x0=x0, tol=1e-10, sensitivities=True)
+    torch.cuda.synchronize()
+    t_gpu = time.time() - t0
+    kern = _class_rates(bpf, ("factor", "trsv"))
+    bpf._lib.set_timing(False)
+
+    class _LU:
+        def refactor(self, vals):
+            J = sp.csc_matrix(sp.csr_matrix((vals, prob.pattern.indices, prob.pattern.indptr),
+                                            shape=prob.pattern.shape))
+            self.lu = spla.splu(J, permc_spec="COLAMD")
+
+        def solve(self, B):
+            return self.lu.solve(np.asarray(B))
+
+    t0 = time.time()
+    rc = NT.newton(prob, solver=_LU(), x0=x0, tol=1e-10, sensitivities=True)
+    t_cpu = time.time() - t0
+    dev_ms = sum(v["ms"] for v in kern.values())
+    line = {"config": {"workload": "grid9k_newton_powerflow_rf", "unknowns": int(prob.pattern.shape[0]),
+                       "controls": int(len(prob.ctrl)), "start": "operating point + N(0, 0.001)",
+                       "tol": 1e-10},
+            "metric": "Newton power flow + sensitivities, seconds", "unit": "s", "higher_is_better": False,
+            "value": t_gpu, "iterations": r.iterations, "converged": bool(r.converged),
+            "residuals": r.residuals, "device_linear_ms": dev_ms, "kernels": kern,
+            "host_ms": 1e3 * t_gpu - dev_ms,
+            "sensitivity_rel_diff_vs_superlu": float(np.linalg.norm(r.sensitivities - rc.sensitivities)
+                                                     / np.linalg.norm(rc.sensitivities)),
+            "cpu_baseline": {"value": t_cpu, "unit": "s", "cores": 1, "kind": "scipy SuperLU in the same loop",
+                             "iterations": rc.iterations},
+            "dtype": "f64", "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
 def batch_workload(nsys=512, seed=0):
     """Fourth configuration's inputs: nsys synthetic grids with log-uniform 100 - 3,000 buses
     and U{8..64} Gaussian right-hand sides each (seeded)."""
@@ -588,12 +644,12 @@ def main():
                     help="iterations the reference arm extrapolates to (the GPU solve's count)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--config", default="headline",
-                    choices=["headline", "gmres300", "bicgstab9k", "rf25k", "batch512"],
+                    choices=["headline", "gmres300", "bicgstab9k", "rf25k", "batch512", "newton9k"],
                     help="the other benchmark configurations (one JSON line each, one GPU)")
     args = ap.parse_args()
     if args.config != "headline":
         {"gmres300": config_gmres300, "bicgstab9k": config_bicgstab9k,
-         "rf25k": config_rf25k, "batch512": config_batch512}[args.config](args)
+         "rf25k": config_rf25k, "batch512": config_batch512, "newton9k": config_newton9k}[args.config](args)
         return
     if args.kernel_only:
         kernel_only(args.kernel_only, args.reps, args.iters, args.ordering)

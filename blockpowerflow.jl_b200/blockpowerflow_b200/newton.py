@@ -1,0 +1,221 @@
+"""Newton power-flow driver: the caller of the multi-RHS solve path.
+
+The reference's solvers serve a Newton power-flow loop (ExaPF produced the benchmark dumps
+Gx / Gu, benchmarks/benchmarks_nvidia.jl:29-39, and the refactorization is its per-step hot call,
+src/cusolverRF.jl:304-314): at every Newton step the Jacobian Gx gets new values on a fixed
+sparsity pattern, is refactored, and the correction is solved; at the solution the sensitivities
+Gx^{-1} Gu of the state to the controls are a multi-RHS solve.  This module is that loop, with
+every linear solve in libbpf.so.
+
+Problem: a grid (grid.Grid) with its operating point taken as the solution: the injections
+S_spec = V conj(Ybus V) at that point fix P at every non-slack bus and Q at every PQ bus; the
+voltage magnitudes of the slack and PV buses and the slack angle are controls.  Unknowns x =
+[theta(non-slack); |V|(PQ)], equations F(x) = [P(non-slack); Q(PQ)] of S(V(x)) - S_spec, Jacobian
+dF/dx = grid.jacobian (the layout of ExaPF's Gx).  Controls u = |V| at the slack and PV buses;
+Gu = dF/du (dense, n x (1 + n_pv)).
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import grid as G
+
+
+@dataclasses.dataclass
+class PowerFlowProblem:
+    grid: G.Grid
+    s_spec: np.ndarray        # complex injections at the solution
+    vm_ctrl: np.ndarray       # |V| of the control buses (slack and PV), in ctrl order
+    ctrl: np.ndarray          # control buses: slack (0) then the PV buses
+    pattern: sp.csr_matrix    # fixed sparsity of Gx over every Newton step
+
+
+def _injections(grid: G.Grid, vm, va) -> np.ndarray:
+    V = vm * np.exp(1j * va)
+    return V * np.conj(grid.ybus() @ V)
+
+
+def make_problem(grid: G.Grid) -> PowerFlowProblem:
+    """The power flow whose solution is the grid's operating point."""
+    s = _injections(grid, grid.vm, grid.va)
+    ctrl = np.concatenate([[0], np.setdiff1d(grid.pv, [0])]).astype(np.int64)
+    # Structural pattern of Gx: the Jacobian at a generic point (no cancellations), so that
+    # every Newton step's values fit it (grid.jacobian_on_pattern checks this).
+    rng = np.random.default_rng(12345)
+    vm_g = grid.vm * (1.0 + 0.01 * rng.standard_normal(grid.n_bus))
+    va_g = grid.va + 0.01 * rng.standard_normal(grid.n_bus)
+    va_g[0] = 0.0
+    pattern = G.jacobian(grid, vm_g, va_g)
+    return PowerFlowProblem(grid, s, grid.vm[ctrl].copy(), ctrl, pattern)
+
+
+def state_to_voltages(prob: PowerFlowProblem, x: np.ndarray):
+    """(vm, va) of every bus from the unknowns x = [theta(non-slack); |V|(PQ)]."""
+    g = prob.grid
+    nb = g.n_bus
+    va = np.zeros(nb)
+    va[1:] = x[:nb - 1]
+    vm = np.empty(nb)
+    vm[prob.ctrl] = prob.vm_ctrl
+    vm[g.pq] = x[nb - 1:]
+    return vm, va
+
+
+def flat_start(prob: PowerFlowProblem) -> np.ndarray:
+    """theta = 0, |V| = 1 at the PQ buses.  (The synthetic grids' operating points are random, with
+    large flows; from the flat start Newton may reach another solution of these lossless networks
+    or stall, so the loop is normally started near the previous operating point.)"""
+    g = prob.grid
+    return np.concatenate([np.zeros(g.n_bus - 1), np.ones(len(g.pq))])
+
+
+def perturbed_start(prob: PowerFlowProblem, sigma: float = 0.01, seed: int = 0) -> np.ndarray:
+    """The solution's state with N(0, sigma) added to every angle and PQ magnitude: the start of
+    a Newton step sequence whose operating point moved by N(0, sigma) (the perturbation of the
+    refactorization benchmark's Jacobian sequence)."""
+    g = prob.grid
+    rng = np.random.default_rng(seed)
+    x = np.concatenate([g.va[1:], g.vm[g.pq]])
+    return x + rng.normal(0.0, sigma, len(x))
+
+
+def mismatch(prob: PowerFlowProblem, x: np.ndarray) -> np.ndarray:
+    """F(x) = [P(non-slack); Q(PQ)] of S(V(x)) - S_spec."""
+    vm, va = state_to_voltages(prob, x)
+    d = _injections(prob.grid, vm, va) - prob.s_spec
+    return np.concatenate([d.real[1:], d.imag[prob.grid.pq]])
+
+
+def jacobian_values(prob: PowerFlowProblem, x: np.ndarray) -> np.ndarray:
+    """Gx's values on the fixed pattern (CSR order)."""
+    vm, va = state_to_voltages(prob, x)
+    return G.jacobian_on_pattern(prob.grid, prob.pattern, vm, va)
+
+
+def control_jacobian(prob: PowerFlowProblem, x: np.ndarray) -> np.ndarray:
+    """Gu = dF/du, u = |V| of the control buses (dense, n_unknowns x n_ctrl):
+    dS/d|V| = diag(V) conj(Ybus diag(V / |V|)) + conj(diag(Ybus V)) diag(V / |V|)."""
+    g = prob.grid
+    vm, va = state_to_voltages(prob, x)
+    Y = g.ybus()
+    V = vm * np.exp(1j * va)
+    I = Y @ V
+    Vn = V / np.abs(V)
+    dS = (sp.diags(V) @ (Y @ sp.diags(Vn)).conj() + sp.diags(I.conj()) @ sp.diags(Vn)).tocsc()
+    cols = dS[:, prob.ctrl].toarray()
+    return np.vstack([cols.real[1:], cols.imag[g.pq]])
+
+
+@dataclasses.dataclass
+class NewtonResult:
+    x: np.ndarray
+    vm: np.ndarray
+    va: np.ndarray
+    iterations: int
+    converged: bool
+    residuals: list            # ||F||_inf before each step and at the end
+    sensitivities: np.ndarray | None = None   # dx/du = -Gx^{-1} Gu at the solution
+
+
+class _RFSolver:
+    """Linear solves of the loop on the cusolverRF-style refactorization: analysis once, then
+    refactor + solve per Newton step; the sensitivities reuse the last factorization."""
+
+    def __init__(self, prob, nrhs, ordering):
+        import torch
+
+        from . import cusolverrf as RF
+        from .sparse import CuSparseMatrixCSR
+
+        self.RF, self.torch = RF, torch
+        self.A = CuSparseMatrixCSR.from_scipy(prob.pattern)
+        self.rf = RF.CusolverRfLU(self.A, nrhs=max(1, nrhs), ordering=ordering)
+
+    def refactor(self, vals):
+        self.A.nzVal.copy_(self.torch.as_tensor(vals, device=self.A.nzVal.device))
+        self.RF.update_(self.rf, self.A)
+
+    def solve(self, B):
+        from .sparse import colmajor
+
+        X = colmajor(self.torch.as_tensor(np.asarray(B, dtype=np.float64).reshape(B.shape[0], -1),
+                                          device=self.A.nzVal.device))
+        X = X.clone()
+        self.RF.ldiv_(self.rf, X)
+        return X.cpu().numpy()
+
+
+class _GmresSolver:
+    """Linear solves of the loop by ILU(0)-preconditioned block-GMRES (refactor per step)."""
+
+    def __init__(self, prob, nrhs, ordering, rtol=1e-12):
+        import torch
+
+        from . import precond
+        from .sparse import CuSparseMatrixCSR
+
+        self.torch = torch
+        self.A = CuSparseMatrixCSR.from_scipy(prob.pattern)
+        self.N = precond.ilu0(self.A, max(1, nrhs), ordering=ordering)
+        self.rtol = rtol
+
+    def refactor(self, vals):
+        self.A.nzVal.copy_(self.torch.as_tensor(vals, device=self.A.nzVal.device))
+        self.N.refactor(self.A.nzVal)
+
+    def solve(self, B):
+        from . import krylov
+
+        B2 = np.asarray(B, dtype=np.float64).reshape(B.shape[0], -1)
+        X, st = krylov.block_gmres(self.A, self.torch.as_tensor(B2, device=self.A.nzVal.device), N=self.N,
+                                   ldiv=True, restart=False, memory=200, atol=0.0, rtol=self.rtol,
+                                   itmax=400)
+        return X.cpu().numpy()
+
+
+def newton(prob: PowerFlowProblem, *, solver="rf", tol: float = 1e-10, maxiter: int = 20,
+           x0: np.ndarray | None = None, sensitivities: bool = False, ordering: str = "AMD",
+           line_search: bool = True) -> NewtonResult:
+    """Newton's method F(x) = 0 from x0 (default: the flat start), stopping at ||F||_inf <= tol;
+    with line_search, a step is halved (down to 2^-12) until ||F||_inf decreases.
+
+    solver: "rf" (refactor + direct solve per step on the device, the reference's per-Newton-
+    step use of CusolverRfLU), "gmres" (ILU(0) refactor + block-GMRES), or an object with
+    refactor(values) and solve(B) methods (a test stand-in for the host logic).  With
+    sensitivities=True, dx/du = -Gx^{-1} Gu at the solution (one multi-RHS solve)."""
+    n_ctrl = len(prob.ctrl)
+    nrhs = n_ctrl if sensitivities else 1
+    if solver == "rf":
+        lin = _RFSolver(prob, nrhs, ordering)
+    elif solver == "gmres":
+        lin = _GmresSolver(prob, nrhs, ordering)
+    else:
+        lin = solver
+    x = flat_start(prob) if x0 is None else np.array(x0, dtype=np.float64)
+    res = []
+    converged = False
+    it = 0
+    for it in range(maxiter + 1):
+        F = mismatch(prob, x)
+        res.append(float(np.abs(F).max()))
+        if res[-1] <= tol:
+            converged = True
+            break
+        if it == maxiter:
+            break
+        lin.refactor(jacobian_values(prob, x))
+        dx = -lin.solve(F[:, None])[:, 0]
+        a = 1.0
+        if line_search:
+            while a > 2.0 ** -12 and np.abs(mismatch(prob, x + a * dx)).max() >= res[-1]:
+                a *= 0.5
+        x = x + a * dx
+    vm, va = state_to_voltages(prob, x)
+    out = NewtonResult(x, vm, va, it, converged, res)
+    if sensitivities and converged:
+        lin.refactor(jacobian_values(prob, x))
+        out.sensitivities = -lin.solve(control_jacobian(prob, x))
+    return out

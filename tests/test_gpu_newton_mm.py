@@ -1,0 +1,66 @@
+"""The callers around the solve path, on the device: the Newton power-flow driver (refactor +
+solve per step, then the multi-RHS sensitivities Gx^{-1} Gu) and the MatrixMarket dump ingest
+with the reference benchmark's solve.
+
+Parity: the Newton iterates of the device solvers against the same loop with SciPy's direct
+solve (iteration counts within one, solutions to 1e-8), the sensitivities to 1e-9 relative (RF) /
+1e-8 (block-GMRES at rtol 1e-12); the dump solve against the fixture's direct solution of the
+reference's own Gx X = Gu (1e-8 relative)."""
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+from scipy.io import mmwrite
+
+from blockpowerflow_b200 import grid as G
+from blockpowerflow_b200 import newton as NT
+from test_newton_host import _SciPyStandIn
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.fixture(scope="module")
+def bpf():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import blockpowerflow_b200 as bpf
+
+    return bpf
+
+
+@pytest.mark.parametrize("n_bus,solver", [(300, "rf"), (2000, "rf"), (300, "gmres"), (2000, "gmres")])
+def test_newton_on_the_device_matches_the_direct_loop(bpf, n_bus, solver):
+    prob = NT.make_problem(G.make_grid(n_bus, seed=7))
+    x0 = NT.perturbed_start(prob, 0.01, seed=2)
+    r = NT.newton(prob, solver=solver, x0=x0, tol=1e-10, sensitivities=True)
+    ref = NT.newton(prob, solver=_SciPyStandIn(prob.pattern), x0=x0, tol=1e-10, sensitivities=True)
+    assert r.converged and ref.converged, (r.residuals, ref.residuals)
+    assert abs(r.iterations - ref.iterations) <= 1, (r.residuals, ref.residuals)
+    np.testing.assert_allclose(r.x, ref.x, rtol=0, atol=1e-8)
+    tol = 1e-9 if solver == "rf" else 1e-8
+    err = np.linalg.norm(r.sensitivities - ref.sensitivities) / np.linalg.norm(ref.sensitivities)
+    assert err <= tol, err
+
+
+def test_dump_ingest_and_the_benchmark_solve(bpf, tmp_path):
+    from blockpowerflow_b200 import mm
+
+    d = np.load(os.path.join(GOLDEN, "dump_case300.npz"))
+    A = sp.csr_matrix((d["data"], d["indices"], d["indptr"]), shape=tuple(d["shape"]))
+    pa, pb = mm.dump_paths(str(tmp_path), "case300")
+    mmwrite(pa, A)
+    mmwrite(pb, sp.coo_matrix(d["Gu"]))
+    Ah, Bh = mm.load_dump(str(tmp_path), "case300")
+    X, st, rn = mm.solve_dump(Ah, Bh, atol=0.0, rtol=1e-12, memory=100, itmax=200)
+    assert st.solved
+    assert np.linalg.norm(X - d["X"]) / np.linalg.norm(d["X"]) <= 1e-8
+    assert abs(rn - np.linalg.norm(Bh - Ah @ X)) <= 1e-12 * max(rn, 1.0)
+    # the script's own parameters (atol 1e-10, rtol 0, memory 1, restart false, itmax 50)
+    X2, st2, rn2 = mm.solve_dump(Ah, Bh)
+    assert st2.niter <= 50 and np.isfinite(rn2)
+    if st2.solved:
+        assert rn2 <= 1e-9, rn2
