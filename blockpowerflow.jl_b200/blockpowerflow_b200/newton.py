@@ -167,13 +167,17 @@ class _GmresSolver:
         self.N.refactor(self.A.nzVal)
 
     def solve(self, B):
+        """block_gmres on slices of at most 128 columns (the widest block it takes)."""
         from . import krylov
 
         B2 = np.asarray(B, dtype=np.float64).reshape(B.shape[0], -1)
-        X, st = krylov.block_gmres(self.A, self.torch.as_tensor(B2, device=self.A.nzVal.device), N=self.N,
-                                   ldiv=True, restart=False, memory=200, atol=0.0, rtol=self.rtol,
-                                   itmax=400)
-        return X.cpu().numpy()
+        out = np.empty_like(B2)
+        for c0 in range(0, B2.shape[1], 128):
+            Bc = self.torch.as_tensor(np.ascontiguousarray(B2[:, c0:c0 + 128]), device=self.A.nzVal.device)
+            X, st = krylov.block_gmres(self.A, Bc, N=self.N, ldiv=True, restart=False, memory=200, atol=0.0,
+                                       rtol=self.rtol, itmax=400)
+            out[:, c0:c0 + 128] = X.cpu().numpy()
+        return out
 
 
 def newton(prob: PowerFlowProblem, *, solver="rf", tol: float = 1e-10, maxiter: int = 20,

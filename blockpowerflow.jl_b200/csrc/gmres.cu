@@ -502,10 +502,78 @@ static bpf_status block_gmres_impl(bpf_ctx *ctx, const bpf_csr_desc *A, int p, c
     return BPF_SUCCESS;
 }
 
+// Blocks wider than the 128 columns one solve takes are solved in column slices of at most 128
+// (nearly equal widths), each by block-GMRES with atol scaled by sqrt(p_s / p): by Minkowski's
+// inequality the slices' residuals then meet ||R||_F <= atol + rtol ||B||_F for the whole block,
+// the reference's test (src/block_gmres.jl:223-231).  itmax defaults to 2 div(n, p) of the whole
+// block.  Stats: niter and npass are the slices' largest, solved = every slice solved, the
+// residual history at iteration k the root-sum-square of the slices' (a finished slice keeps its
+// last value), timer the sum.
+static bpf_status block_gmres_sliced(bpf_ctx *ctx, const bpf_csr_desc *A, int p, const double *B, int ldb,
+                                     double *X, int ldx, const double *X0, int ldx0, const bpf_prec *M,
+                                     const bpf_prec *N, const bpf_gmres_opts *opts, bpf_stats *stats) {
+    const int ns = (p + 127) / 128;
+    const int n = A->n;
+    bpf_gmres_opts o = *opts;
+    if (o.itmax == 0) o.itmax = std::max(1, 2 * (n / p));
+    const int cap = o.itmax + 2;
+    std::vector<std::vector<double>> hist(ns, std::vector<double>(cap, 0.0));
+    std::vector<int> nres(ns, 0);
+    int niter = 0, npass = 0, solved = 1, status = BPF_SOLVE_SOLVED;
+    double timer = 0.0;
+    int c0 = 0;
+    for (int k = 0; k < ns; k++) {
+        const int q = p / ns + (k < p % ns ? 1 : 0);
+        bpf_gmres_opts os = o;
+        os.atol = o.atol * std::sqrt((double)q / (double)p);
+        if (o.timemax > 0.0 && o.timemax < 1e300) os.timemax = std::max(1e-9, o.timemax - timer);
+        bpf_stats st{};
+        st.residuals_capacity = cap;
+        st.residuals = hist[k].data();
+        bpf_status r = block_gmres_impl(ctx, A, q, B + (size_t)c0 * ldb, ldb, X + (size_t)c0 * ldx, ldx,
+                                        X0 ? X0 + (size_t)c0 * ldx0 : nullptr, ldx0, M, N, &os, &st, nullptr, 0, 0);
+        if (r != BPF_SUCCESS) return r;
+        niter = std::max(niter, st.niter);
+        npass = std::max(npass, st.npass);
+        timer += st.timer;
+        nres[k] = std::min(st.n_residuals, cap);
+        if (!st.solved) {
+            solved = 0;
+            if (st.status == BPF_SOLVE_TIMEMAX || status == BPF_SOLVE_TIMEMAX) status = BPF_SOLVE_TIMEMAX;
+            else status = st.status;
+        }
+        c0 += q;
+    }
+    if (stats) {
+        stats->niter = niter;
+        stats->solved = solved;
+        stats->status = status;
+        stats->timer = timer;
+        stats->npass = npass;
+        int nr = 0;
+        for (int k = 0; k < ns; k++) nr = std::max(nr, nres[k]);
+        stats->n_residuals = nr;
+        if (stats->residuals && stats->residuals_capacity > 0) {
+            for (int i = 0; i < std::min(nr, stats->residuals_capacity); i++) {
+                double s2 = 0.0;
+                for (int k = 0; k < ns; k++) {
+                    if (nres[k] == 0) continue;
+                    const double v = hist[k][std::min(i, nres[k] - 1)];
+                    s2 += v * v;
+                }
+                stats->residuals[i] = std::sqrt(s2);
+            }
+        }
+    }
+    return BPF_SUCCESS;
+}
+
 extern "C" bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p, const double *B,
                                       int ldb, double *X, int ldx, const double *X0, int ldx0,
                                       const bpf_prec *M, const bpf_prec *N, const bpf_gmres_opts *opts,
                                       bpf_stats *stats) {
+    if (ctx && A && opts && B && X && p > 128 && p <= A->n)
+        return block_gmres_sliced(ctx, A, p, B, ldb, X, ldx, X0, ldx0, M, N, opts, stats);
     return block_gmres_impl(ctx, A, p, B, ldb, X, ldx, X0, ldx0, M, N, opts, stats, nullptr, 0, 0);
 }
 

@@ -261,7 +261,10 @@ BPF_API bpf_status bpf_prec_destroy(bpf_prec *prec);
 
 /* ---- block Krylov solvers -------------------------------------------------------------- */
 /* block_gmres(A, B[, X0]; kwargs...) -> (X, stats): src/block_gmres.jl:127-154,170-411.
- * X0 nullable (warm start).  M: left, N: right preconditioner, either nullable (= I). */
+ * X0 nullable (warm start).  M: left, N: right preconditioner, either nullable (= I).
+ * p > 128: solved in column slices of at most 128, each by block-GMRES with atol scaled by
+ * sqrt(p_slice / p), so the whole block still meets ||R||_F <= atol + rtol ||B||_F; stats give
+ * the largest slice iteration count and the root-sum-square residual history. */
 BPF_API bpf_status bpf_block_gmres(bpf_ctx *ctx, const bpf_csr_desc *A, int p,
                                    const double *B, int ldb, double *X, int ldx,
                                    const double *X0, int ldx0, const bpf_prec *M,

@@ -151,6 +151,23 @@ def test_gmres_benchmark_dump_case300(dump300, bpf):
     assert np.linalg.norm(X.cpu().numpy() - Xd) <= 1e-9 * np.linalg.norm(Xd)
 
 
+def test_gmres_wide_block_of_the_benchmark_dump(dump300, bpf):
+    """All 137 sensitivity RHS of the reference's case300 dump in one call (the benchmark
+    script's block): wider than one solve's 128 columns, so the entry point solves column
+    slices; the block still meets ||R||_F <= atol + rtol ||B||_F and matches the direct solve."""
+    Gx, z = dump300
+    Gu = z["Gu"]
+    assert Gu.shape[1] > 128
+    Ad = _dev(Gx, bpf)
+    X, st = bpf.block_gmres(Ad, _t(Gu), N=bpf.ilu0(Ad, Gu.shape[1]), ldiv=True, memory=8, restart=True,
+                            atol=0.0, rtol=1e-13, itmax=400, history=True)
+    assert st.solved
+    Xh = X.cpu().numpy()
+    assert np.linalg.norm(Gu - Gx @ Xh) <= 1e-12 * np.linalg.norm(Gu)
+    assert np.linalg.norm(Xh - z["X"]) <= 1e-9 * np.linalg.norm(z["X"])
+    assert len(st.residuals) >= 2 and st.residuals[-1] <= st.residuals[0]
+
+
 @pytest.mark.parametrize("n_bus,p", [(300, 16), (1000, 64)])
 def test_gmres_fp32_factors_flexible_reaches_fp64_residual(bpf, n_bus, p):
     """Mixed precision: FP32 ILU0 factors and triangular solves inside FP64 flexible GMRES.
