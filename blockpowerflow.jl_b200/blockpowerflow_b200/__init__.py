@@ -11,7 +11,7 @@ from .batch import BatchPlan, BatchStats, autotune
 from ._lib import (BPFError, DimensionMismatch, SingularException, exported_symbols,
                    kernel_launches)
 from .krylov import BlockGMRESStats, SimpleStats, block_bicgstab, block_gmres
-from .precond import NVIDIA_IC0, NVIDIA_ILU0, ic0, ilu0, ldiv_
+from .precond import NVIDIA_IC0, NVIDIA_ILU0, BlockJacobiPreconditioner, ic0, ilu0, ldiv_, mul_
 from .sparse import CuSparseMatrixCSR, colmajor, empty_colmajor, householder, mul
 
 ldiv = ldiv_
@@ -21,4 +21,5 @@ __all__ = [
     "ldiv", "NVIDIA_ILU0", "NVIDIA_IC0", "CuSparseMatrixCSR", "mul", "householder", "colmajor",
     "empty_colmajor", "BPFError", "DimensionMismatch", "SingularException", "grid",
     "exported_symbols", "kernel_launches", "CUSOLVERRF", "BatchPlan", "BatchStats", "autotune",
+    "BlockJacobiPreconditioner", "mul_",
 ]

@@ -93,6 +93,7 @@ SIGNATURES = {
     "bpf_ilu0_create_ordered": (_I, [_P, C.POINTER(CsrDesc), _I, _I, _I, C.POINTER(_P)]),
     "bpf_ic0_create_ordered": (_I, [_P, C.POINTER(CsrDesc), _I, _I, _I, C.POINTER(_P)]),
     "bpf_prec_permutation": (_I, [_P, _P]),
+    "bpf_block_jacobi_create": (_I, [_P, C.POINTER(CsrDesc), _I, _I, C.POINTER(_P)]),
     "bpf_tc_gemm_bf16": (_I, [_P, _I, _I, _I, _P, _I, _P, _I, _P, _I, _I, _I]),
     "bpf_mlp_create": (_I, [_P, _I, _I, C.c_ulonglong, C.POINTER(_P)]),
     "bpf_mlp_destroy": (_I, [_P]),

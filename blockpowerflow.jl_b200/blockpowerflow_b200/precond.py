@@ -1,4 +1,5 @@
-"""ILU(0) / IC(0) preconditioners: ilu0, ic0, ldiv! (src/preconditioners_nvidia.jl)."""
+"""ILU(0) / IC(0) preconditioners: ilu0, ic0, ldiv! (src/preconditioners_nvidia.jl); and the
+block-Jacobi preconditioner the reference's tests use (ExaPF's BlockJacobiPreconditioner)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -125,4 +126,75 @@ def ldiv_(y, P: _DevicePrec, x):
         raise ValueError("y must be column-major (Fortran order)")
     _lib.check(_lib.load().bpf_prec_apply(P.handle, p, xc.data_ptr(), ld(xc), yc.data_ptr(),
                                           ld(yc)), P._ctx)
+    return y
+
+
+class BlockJacobiPreconditioner:
+    """ExaPF's LinearSolvers.BlockJacobiPreconditioner(A, nblocks, device) as the reference's
+    tests and benchmark use it (test/block_gmres.jl:5,17,22; benchmarks_nvidia.jl:47-51): the
+    dense inverses of the diagonal blocks, applied by mul! (y = P x), so block_gmres takes it with
+    ldiv=False.  Blocks are consecutive runs of block_size rows (default: ceil(n / nblocks), at
+    most 32) in `ordering` (ExaPF partitions with METIS, which is not available here).
+    update(A) recomputes the inverses from A's current values (ExaPF's LS.update)."""
+
+    kind = "block_jacobi"
+
+    def __init__(self, A: CuSparseMatrixCSR, nblocks: int | None = None, *, block_size: int | None = None,
+                 ordering: str = "natural"):
+        n = A.n
+        if block_size is None:
+            nb = max(1, int(nblocks)) if nblocks else max(1, n // 32)
+            block_size = min(32, -(-n // nb))
+        key = ordering.lstrip(":").upper() if isinstance(ordering, str) else ordering
+        if key not in _lib.ORDERINGS:
+            raise ValueError(f"unknown ordering {ordering!r}")
+        self.A, self.n, self.block_size, self.ordering = A, n, int(block_size), key
+        lib = _lib.load()
+        self._ctx = _lib.context(A.nzVal.device.index)
+        h = C.c_void_p()
+        d = A.desc()
+        _lib.check(lib.bpf_block_jacobi_create(self._ctx, C.byref(d), self.block_size, _lib.ORDERINGS[key],
+                                               C.byref(h)), self._ctx)
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def order(self):
+        """The row order the blocks are cut from."""
+        import numpy as np
+
+        p = np.zeros(self.n, dtype=np.int32)
+        _lib.check(_lib.load().bpf_prec_permutation(self._h, p.ctypes.data_as(C.c_void_p)), self._ctx)
+        return p
+
+    def update(self, A: CuSparseMatrixCSR | None = None) -> None:
+        A = self.A if A is None else A
+        _lib.check(_lib.load().bpf_prec_refactor(self._h, C.c_void_p(A.nzVal.data_ptr())), self._ctx)
+
+    def mul(self, x):
+        """y = P x (a new column-major block)."""
+        xc = colmajor(x)
+        y = empty_colmajor(xc.shape[0], xc.shape[1], xc.device)
+        return mul_(y, self, xc)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                _lib.load().bpf_prec_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+def mul_(y, P: BlockJacobiPreconditioner, x):
+    """mul!(y, P, x): y = P x for the block-Jacobi preconditioner."""
+    xc = colmajor(x)
+    n, p = xc.shape
+    if n != P.n or tuple(y.shape) != (n, p) or y.stride(0) != 1:
+        raise _lib.DimensionMismatch(_lib.BPF_ERR_DIMENSION, "Inconsistent problem size")
+    _lib.check(_lib.load().bpf_prec_apply(P.handle, p, xc.data_ptr(), ld(xc), y.data_ptr(), ld(y)), P._ctx)
     return y

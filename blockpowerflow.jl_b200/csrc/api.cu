@@ -488,6 +488,10 @@ bpf_status bpf_prec_refactor(bpf_prec *P, const double *vals) {
     bpf_ctx *ctx = P->ctx;
     if (P->nnz > 0 && !vals) return set_error(ctx, BPF_ERR_INVALID_VALUE, "null values");
     BPF_TRY(prec_load_values(ctx, P, vals));
+    if (P->kind == PREC_BJ) {
+        BPF_TRY(bj_setup(ctx, P));
+        return check_dev_status(ctx, "block-Jacobi (singular diagonal block)");
+    }
     BPF_TRY(factor_numeric(ctx, P));
     BPF_TRY(tri_scatter(ctx, P->lower, P->fv));
     BPF_TRY(tri_scatter(ctx, P->upper, P->fv));
@@ -520,6 +524,8 @@ bpf_status bpf_prec_apply(bpf_prec *P, int p, const double *X, int ldx, double *
 bpf_status bpf_prec_factor_values(const bpf_prec *P, double *vals) {
     if (!P || (P->nnz > 0 && !vals)) return BPF_ERR_INVALID_VALUE;
     bpf_ctx *ctx = P->ctx;
+    if (P->kind == PREC_BJ)
+        return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "block-Jacobi holds dense block inverses, not factors on A's pattern");
     if (P->nnz > 0)
         BPF_CUDA(ctx, cudaMemcpyAsync(vals, P->fv, sizeof(double) * P->nnz, cudaMemcpyDeviceToDevice,
                                       ctx->stream));
@@ -550,6 +556,10 @@ bpf_status bpf_prec_destroy(bpf_prec *P) {
     cudaFree(P->zbuf);
     cudaFree(P->cl_lev_ptr);
     cudaFree(P->cl_ent);
+    cudaFree(P->bj_rows);
+    cudaFree(P->bj_blk);
+    cudaFree(P->bj_loc);
+    cudaFree(P->bj_inv);
     for (int w = 0; w < 2; w++) {
         cudaFree(P->ps_ptr[w]);
         cudaFree(P->ps_src[w]);

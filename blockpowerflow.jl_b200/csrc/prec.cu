@@ -628,6 +628,7 @@ static bpf_status trsv2_dispatch(bpf_ctx *ctx, const TriDev &t0, const TriDev &t
 bpf_status prec_apply_rowmajor(bpf_ctx *ctx, const bpf_prec *P, int p, const double *X,
                                double *Y, const int *gate) {
     if (P->n == 0 || p == 0) return BPF_SUCCESS;
+    if (P->kind == PREC_BJ) return bj_apply_rowmajor(ctx, P, p, X, Y);   // mul! semantics
     if (P->perm && p > P->zcols)
         return set_error(ctx, BPF_ERR_NOT_SUPPORTED,
                          "reordered preconditioner: %d right-hand sides exceed the %d-column scratch "

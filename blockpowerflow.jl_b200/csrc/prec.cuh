@@ -61,7 +61,7 @@ struct TriDev {
     }
 };
 
-enum PrecKind { PREC_ILU0 = 1, PREC_IC0 = 2, PREC_LU = 3 };
+enum PrecKind { PREC_ILU0 = 1, PREC_IC0 = 2, PREC_LU = 3, PREC_BJ = 4 };
 
 TriHost build_tri(int n, const int *rp, const int *ci, const int *diag, int part, bool unit);
 void build_pairs(int n, const int *rp, const int *ci, const int *diag, bool ic,
@@ -103,6 +103,11 @@ struct bpf_prec {
     std::vector<int> perm_host;
     double *zbuf = nullptr;
     int zcols = 0;
+    // Block-Jacobi (bpf_block_jacobi_create): rows of each block (nblk x 32, -1 padded), block and
+    // local index of every row, dense inverses (nblk x 32 x 32); fv holds A's values.
+    int bj_nblk = 0, bj_bs = 0;
+    int *bj_rows = nullptr, *bj_blk = nullptr, *bj_loc = nullptr;
+    double *bj_inv = nullptr;
 };
 
 namespace bpf {
@@ -118,6 +123,9 @@ bpf_status prec_apply_rowmajor(bpf_ctx *ctx, const bpf_prec *P, int p, const dou
 bpf_status prec_reserve_z(bpf_ctx *ctx, bpf_prec *P, int p);
 // A's values into the factor storage (a copy, or the scatter through amap when reordered).
 bpf_status prec_load_values(bpf_ctx *ctx, bpf_prec *P, const double *vals);
+// Block-Jacobi: inverses of the diagonal blocks from fv; Y = P X (row-major, Y may be X).
+bpf_status bj_setup(bpf_ctx *ctx, bpf_prec *P);
+bpf_status bj_apply_rowmajor(bpf_ctx *ctx, const bpf_prec *P, int p, const double *X, double *Y);
 // Y = U^{-1} L^{-1} Y in place (row-major n x p, p <= 256) for an LU factor with push lists.
 bpf_status lu_solve_push_rowmajor(bpf_ctx *ctx, const bpf_prec *P, int p, double *Y);
 }  // namespace bpf

@@ -259,6 +259,17 @@ BPF_API bpf_status bpf_prec_factor_values(const bpf_prec *prec, double *vals);
 BPF_API bpf_status bpf_prec_levels(const bpf_prec *prec, int *levels_lower, int *levels_upper);
 BPF_API bpf_status bpf_prec_destroy(bpf_prec *prec);
 
+/* Block-Jacobi preconditioner (ExaPF's LinearSolvers.BlockJacobiPreconditioner, used by
+ * test/block_gmres.jl:5,17,22 and benchmarks/benchmarks_nvidia.jl:47-51; ExaPF is not part of the
+ * reference): the dense inverses of the diagonal blocks of A, applied by multiplication, y = P x
+ * (mul! semantics: bpf_prec_apply multiplies; block_gmres takes it with ldiv = false).  Blocks are
+ * consecutive runs of block_size (1..32) rows in `ordering` (BPF_ORDER_NATURAL, _RCM, _AMD or
+ * _MDQ; ExaPF's METIS partition is not available: _METIS returns BPF_ERR_NOT_SUPPORTED).
+ * bpf_prec_refactor recomputes the inverses from new values; a singular block returns
+ * BPF_ERR_SINGULAR. */
+BPF_API bpf_status bpf_block_jacobi_create(bpf_ctx *ctx, const bpf_csr_desc *A, int block_size,
+                                           int ordering, bpf_prec **prec);
+
 /* ---- block Krylov solvers -------------------------------------------------------------- */
 /* block_gmres(A, B[, X0]; kwargs...) -> (X, stats): src/block_gmres.jl:127-154,170-411.
  * X0 nullable (warm start).  M: left, N: right preconditioner, either nullable (= I).

@@ -235,3 +235,21 @@ class DenseLU:
         lib().orc_lu_solve(self.n, _ptr(self.LU), _ptr(self.perm, C.c_int), X.shape[1], _ptr(X),
                            self.n)
         return X
+
+
+def block_jacobi_apply(A, order, block_size, X):
+    """Block-Jacobi y = P x with P = diag(A_b^{-1}), the blocks A_b = A(rows_b, rows_b) over
+    consecutive runs of block_size rows of `order`: the algorithm of ExaPF 0.9.3's
+    LinearSolvers.BlockJacobiPreconditioner (dense inverse of every diagonal block, applied by
+    mul!), which the reference's tests and benchmark build (test/block_gmres.jl:5,17,22,
+    benchmarks/benchmarks_nvidia.jl:47-51).  ExaPF's METIS partition is replaced by the given
+    order, as in the library.  Dense LAPACK solves of the small blocks (numpy)."""
+    A = sp.csr_matrix(A)
+    X = np.asarray(X, dtype=np.float64)
+    Y = np.zeros_like(X)
+    order = np.asarray(order)
+    for b0 in range(0, len(order), block_size):
+        rows = order[b0:b0 + block_size]
+        Ab = A[rows][:, rows].toarray()
+        Y[rows] = np.linalg.solve(Ab, X[rows])
+    return Y
