@@ -13,7 +13,7 @@ using CUDA.CUSPARSE
 
 import LinearAlgebra: ldiv!
 
-export block_gmres, block_bicgstab, ilu0, ic0, CUSOLVERRF, BatchPlan, batch_solve!
+export block_gmres, block_bicgstab, ilu0, ic0, CUSOLVERRF, BatchPlan, batch_solve!, BlockJacobiPreconditioner
 
 const libbpf = joinpath(@__DIR__, "..", "lib", "libbpf.so")
 
@@ -150,9 +150,40 @@ function ldiv!(y::CuVecOrMat{Float64}, P::DevicePrec, x::CuVecOrMat{Float64})
     return y
 end
 
+# ---- block-Jacobi (ExaPF's LS.BlockJacobiPreconditioner as test/block_gmres.jl:5 uses it) ------
+mutable struct BlockJacobiPreconditioner
+    h::Ptr{Cvoid}
+    n::Int
+end
+
+function BlockJacobiPreconditioner(A::CuSparseMatrixCSR{Float64,Cint}, nblocks::Int; ordering=:natural)
+    n = size(A, 1)
+    bs = min(32, cld(n, max(nblocks, 1)))
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:bpf_block_jacobi_create, libbpf), Cint,
+                (Ptr{Cvoid}, Ref{CsrDesc}, Cint, Cint, Ref{Ptr{Cvoid}}),
+                ctx(), Ref(desc(A)), bs, PREC_ORDER[ordering], r))
+    P = BlockJacobiPreconditioner(r[], n)
+    finalizer(p -> ccall((:bpf_prec_destroy, libbpf), Cint, (Ptr{Cvoid},), p.h), P)
+    return P
+end
+
+# ExaPF's LS.update(BJ, A, device): the block inverses from A's current values
+update(P::BlockJacobiPreconditioner, A::CuSparseMatrixCSR{Float64,Cint}) =
+    check(ccall((:bpf_prec_refactor, libbpf), Cint, (Ptr{Cvoid}, CuPtr{Cdouble}), P.h, pointer(A.nzVal)))
+
+# mul!(y, P, x): y = P x
+function LinearAlgebra.mul!(y::CuVecOrMat{Float64}, P::BlockJacobiPreconditioner, x::CuVecOrMat{Float64})
+    check(ccall((:bpf_prec_apply, libbpf), Cint,
+                (Ptr{Cvoid}, Cint, CuPtr{Cdouble}, Cint, CuPtr{Cdouble}, Cint),
+                P.h, size(x, 2), pointer(x), stride(x, 2), pointer(y), stride(y, 2)))
+    return y
+end
+
 # ---- block-GMRES (src/block_gmres.jl:127-154) -----------------------------------------
 _handle(::typeof(I)) = C_NULL
 _handle(P::DevicePrec) = P.h
+_handle(P::BlockJacobiPreconditioner) = P.h
 
 function block_gmres(A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64},
                      X0::Union{Nothing,CuMatrix{Float64}}=nothing; memory::Int=20, M=I, N=I,
