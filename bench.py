@@ -18,8 +18,9 @@ Newton loop would.  RHS solves/s = converged right-hand sides / time.
           cores, first iterations of the same solve, scaled to the whole solve by operation
           count.
 
-`--impl reference` times that CPU restatement alone (the reference is Julia and cannot run
-here) on the same workload and prints the same metric with "impl":"reference".
+`--impl reference` times that CPU restatement alone (the reference is Julia, and neither Julia
+nor its CUDA.jl stack is installed) on the same workload and prints the same metric with
+"impl":"reference".
 Multi-GPU (torchrun): every rank solves its own grid (seed offset by rank), no collective on
 the data path; value = all ranks' converged RHS / max-over-ranks time ("scaling": "weak").
 """
