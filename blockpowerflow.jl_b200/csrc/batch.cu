@@ -339,6 +339,7 @@ __device__ void spmm_t(const int *__restrict__ rp, const int *__restrict__ ci, c
                 a = __ldg(av + k);
             }
             const int cnt = min(kG, re - kb);
+            #pragma unroll 4   // several entries' loads in flight; same summation order
             for (int e = 0; e < cnt; e++) {
                 const int cs = __shfl_sync(gmask, col, e, kG);
                 const double as = __shfl_sync(gmask, a, e, kG);
@@ -398,6 +399,7 @@ __device__ void trsv_t(const TriKernelArgs &T, int q, const double *X, double *Y
                     a = val[k];
                 }
                 const int cnt = min(kG, re - kb);
+                #pragma unroll 4   // several entries' loads in flight; same summation order
                 for (int e = 0; e < cnt; e++) {
                     const int cs = __shfl_sync(gmask, col, e, kG);
                     const TF as = __shfl_sync(gmask, a, e, kG);

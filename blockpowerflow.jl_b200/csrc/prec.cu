@@ -545,6 +545,7 @@ trsv2_coop_kernel(TriKernelArgs t0, TriKernelArgs t1, int p, const void *Xv, voi
                     const int cnt = min(G, re - kb);
                     int co = 0;
                     if (k < re && perm && phase == 1) co = __ldg(perm + c);
+                    #pragma unroll 4   // several entries' loads in flight; same summation order
                     for (int s = 0; s < cnt; s++) {
                         const int cs = __shfl_sync(gmask, (perm && phase == 1) ? co : c, s, G);
                         const TF as = __shfl_sync(gmask, a, s, G);

@@ -43,6 +43,7 @@ spmm_rm_kernel(int n, const int *__restrict__ rp, const int *__restrict__ ci,
                 a = __ldg(av + k);
             }
             const int cnt = min(G, re - kb);
+            #pragma unroll 4   // several entries' loads in flight; same summation order
             for (int t = 0; t < cnt; t++) {
                 const int ct = __shfl_sync(gmask, c, t, G);
                 const double at = __shfl_sync(gmask, a, t, G);
