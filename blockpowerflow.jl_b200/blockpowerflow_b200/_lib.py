@@ -131,6 +131,11 @@ SIGNATURES = {
     "bpf_batch_unit_cycles": (_I, [_P, _P]),
     "bpf_batch_info": (_I, [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(C.c_longlong)]),
     "bpf_batch_destroy": (_I, [_P]),
+    "bpf_pf_create": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, C.POINTER(CsrDesc), C.POINTER(_P)]),
+    "bpf_pf_info": (_I, [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),
+    "bpf_pf_mismatch": (_I, [_P, _P, _P, _D, _P, _P, C.POINTER(_D)]),
+    "bpf_pf_jacobian": (_I, [_P, _P, _P, _P, _I]),
+    "bpf_pf_destroy": (_I, [_P]),
 }
 
 _lib = None
@@ -208,7 +213,8 @@ def kernel_launches(device=None) -> int:
 
 
 KERNEL_CLASSES = {"spmm": 0, "trsv": 1, "factor": 2, "gram": 3, "tsmm": 4, "small": 5,
-                  "chol": 6, "hess": 7, "backsub": 8, "mlp": 9, "batch": 10}
+                  "chol": 6, "hess": 7, "backsub": 8, "mlp": 9, "batch": 10,
+                  "pf": 11}
 
 
 def set_timing(on: bool, device=None) -> None:

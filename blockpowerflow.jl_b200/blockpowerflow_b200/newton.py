@@ -5,7 +5,8 @@ Gx / Gu, benchmarks/benchmarks_nvidia.jl:29-39, and the refactorization is its p
 src/cusolverRF.jl:304-314): at every Newton step the Jacobian Gx gets new values on a fixed
 sparsity pattern, is refactored, and the correction is solved; at the solution the sensitivities
 Gx^{-1} Gu of the state to the controls are a multi-RHS solve.  This module is that loop, with
-every linear solve in libbpf.so.
+every linear solve in libbpf.so and, with the device solvers, the mismatch, Gx and Gu assembled
+there too (bpf_pf_*), so that only max |F| crosses to the host per evaluation.
 
 Problem: a grid (grid.Grid) with its operating point taken as the solution: the injections
 S_spec = V conj(Ybus V) at that point fix P at every non-slack bus and Q at every PQ bus; the
@@ -109,6 +110,105 @@ def control_jacobian(prob: PowerFlowProblem, x: np.ndarray) -> np.ndarray:
     return np.vstack([cols.real[1:], cols.imag[g.pq]])
 
 
+def bus_arrays(prob: PowerFlowProblem):
+    """The host arguments of bpf_pf_create for this problem, in its order: Ybus row pointers,
+    columns and interleaved (re, im) values (sorted, duplicates summed), bus types (1 PQ, 2 PV,
+    3 slack), |V| and angle where they are fixed, interleaved specified injections."""
+    g = prob.grid
+    nb = g.n_bus
+    bus_type = np.ones(nb, dtype=np.int32)
+    bus_type[prob.ctrl] = 2
+    bus_type[0] = 3
+    # the problem's layout: slack bus 0, PV controls and PQ unknowns in bus order
+    if (prob.ctrl[0] != 0 or np.any(np.diff(prob.ctrl[1:]) <= 0) or np.any(np.diff(g.pq) <= 0)
+            or not np.array_equal(np.flatnonzero(bus_type == 1), g.pq)):
+        raise ValueError("power flow: buses must be slack 0, then PV / PQ sets in bus order")
+    Y = g.ybus().tocsr()
+    Y.sum_duplicates()
+    Y.sort_indices()
+    vm_fixed = np.ones(nb)
+    vm_fixed[prob.ctrl] = prob.vm_ctrl
+    return [np.ascontiguousarray(Y.indptr, dtype=np.int32),
+            np.ascontiguousarray(Y.indices, dtype=np.int32),
+            np.ascontiguousarray(np.column_stack([Y.data.real, Y.data.imag]).ravel()),
+            bus_type, vm_fixed, np.zeros(nb),
+            np.ascontiguousarray(np.column_stack([prob.s_spec.real, prob.s_spec.imag]).ravel())]
+
+
+class DeviceAssembly:
+    """F, Gx and Gu of a problem assembled on the device (bpf_pf_create / _mismatch / _jacobian):
+    the same quantities as mismatch(), jacobian_values() and control_jacobian(), with Gx written
+    straight into the values of the solver's matrix A (its pattern is prob.pattern)."""
+
+    def __init__(self, prob: PowerFlowProblem, A):
+        import ctypes as C
+
+        from . import _lib
+
+        nb = prob.grid.n_bus
+        self._keep = bus_arrays(prob)
+        self.A = A
+        self._device = A.nzVal.device
+        self._dev = A.nzVal.device.index
+        self._ctx = _lib.context(self._dev)
+        self._lib = _lib
+        h = C.c_void_p()
+        d = A.desc()
+        ptr = [a.ctypes.data for a in self._keep]
+        _lib.check(_lib.load().bpf_pf_create(self._ctx, nb, *ptr, C.byref(d), C.byref(h)), self._ctx)
+        self._h = h
+        n, nc = C.c_int(), C.c_int()
+        _lib.check(_lib.load().bpf_pf_info(h, C.byref(n), C.byref(nc), None), self._ctx)
+        self.n, self.n_ctrl = n.value, nc.value
+
+    def mismatch(self, x, F, dx=None, alpha=0.0, x_out=None) -> float:
+        """F = F(x + alpha dx) (device tensors; x_out, if given, receives that point);
+        returns max |F|."""
+        import ctypes as C
+
+        for v in (x, F, dx, x_out):
+            if v is not None:
+                self._check_vector(v)
+        self._ctx = self._lib.context(self._dev)    # bound to torch's current stream
+        nrm = C.c_double()
+        self._lib.check(self._lib.load().bpf_pf_mismatch(
+            self._h, x.data_ptr(), None if dx is None else dx.data_ptr(), float(alpha),
+            None if x_out is None else x_out.data_ptr(), F.data_ptr(), C.byref(nrm)), self._ctx)
+        return nrm.value
+
+    def _check_vector(self, v):
+        import torch
+
+        if v.dtype != torch.float64 or v.device != self._device or v.numel() != self.n or not v.is_contiguous():
+            raise ValueError(f"power flow: expected a contiguous float64 vector of {self.n} entries on "
+                             f"{self._device}")
+
+    def jacobian(self, x, Gu=None) -> None:
+        """Gx at x into A.nzVal; Gu (column-major n x n_ctrl device block), if given, = dF/du."""
+        import torch
+
+        self._check_vector(x)
+        ld = 0 if Gu is None else (Gu.stride(1) if Gu.shape[1] > 1 else Gu.shape[0])
+        if Gu is not None and (Gu.dtype != torch.float64 or Gu.device != self._device or Gu.dim() != 2
+                               or Gu.stride(0) != 1 or tuple(Gu.shape) != (self.n, self.n_ctrl)
+                               or ld < self.n):
+            raise ValueError("Gu must be a column-major float64 n x n_ctrl block on the matrix's device")
+        if self.A.nzVal.numel() != self.A.nnz:
+            raise ValueError("power flow: the matrix's values changed size")
+        self._ctx = self._lib.context(self._dev)
+        self._lib.check(self._lib.load().bpf_pf_jacobian(
+            self._h, x.data_ptr(), self.A.nzVal.data_ptr(), None if Gu is None else Gu.data_ptr(), ld),
+            self._ctx)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                self._lib.load().bpf_pf_destroy(h)
+            except Exception:
+                pass
+
+
 @dataclasses.dataclass
 class NewtonResult:
     x: np.ndarray
@@ -147,6 +247,18 @@ class _RFSolver:
         self.RF.ldiv_(self.rf, X)
         return X.cpu().numpy()
 
+    def refactor_device(self):
+        """Refactor from the values already in A.nzVal."""
+        self.RF.update_(self.rf, self.A)
+
+    def solve_device(self, B, X=None):
+        """X = Gx^{-1} B for a column-major device block B (X: a like-shaped block, or in place)."""
+        X = B if X is None else X
+        if X.data_ptr() != B.data_ptr():
+            X.copy_(B)
+        self.RF.ldiv_(self.rf, X)
+        return X
+
 
 class _GmresSolver:
     """Linear solves of the loop by ILU(0)-preconditioned block-GMRES (refactor per step)."""
@@ -179,6 +291,21 @@ class _GmresSolver:
             out[:, c0:c0 + 128] = X.cpu().numpy()
         return out
 
+    def refactor_device(self):
+        self.N.refactor(self.A.nzVal)
+
+    def solve_device(self, B, X=None):
+        """X = Gx^{-1} B for a column-major device block B, by slices of at most 128 columns."""
+        from . import krylov
+
+        X = self.torch.empty_like(B) if X is None or X.data_ptr() == B.data_ptr() else X
+        Bm, Xm = B.reshape(B.shape[0], -1), X.reshape(X.shape[0], -1)
+        for c0 in range(0, Bm.shape[1], 128):
+            Xc, st = krylov.block_gmres(self.A, Bm[:, c0:c0 + 128], N=self.N, ldiv=True, restart=False,
+                                        memory=200, atol=0.0, rtol=self.rtol, itmax=400)
+            Xm[:, c0:c0 + 128].copy_(Xc)
+        return X
+
 
 def newton(prob: PowerFlowProblem, *, solver="rf", tol: float = 1e-10, maxiter: int = 20,
            x0: np.ndarray | None = None, sensitivities: bool = False, ordering: str = "AMD",
@@ -188,8 +315,10 @@ def newton(prob: PowerFlowProblem, *, solver="rf", tol: float = 1e-10, maxiter: 
 
     solver: "rf" (refactor + direct solve per step on the device, the reference's per-Newton-
     step use of CusolverRfLU), "gmres" (ILU(0) refactor + block-GMRES), or an object with
-    refactor(values) and solve(B) methods (a test stand-in for the host logic).  With
-    sensitivities=True, dx/du = -Gx^{-1} Gu at the solution (one multi-RHS solve)."""
+    refactor(values) and solve(B) methods (a host stand-in: then F, Gx and Gu are assembled by
+    numpy).  With "rf" / "gmres" the mismatch, Gx and Gu are assembled on the device
+    (DeviceAssembly) and x, F and the steps stay there.  With sensitivities=True, dx/du =
+    -Gx^{-1} Gu at the solution (one multi-RHS solve)."""
     n_ctrl = len(prob.ctrl)
     nrhs = n_ctrl if sensitivities else 1
     if solver == "rf":
@@ -198,6 +327,8 @@ def newton(prob: PowerFlowProblem, *, solver="rf", tol: float = 1e-10, maxiter: 
         lin = _GmresSolver(prob, nrhs, ordering)
     else:
         lin = solver
+    if hasattr(lin, "solve_device"):
+        return _newton_device(prob, lin, tol, maxiter, x0, sensitivities, line_search)
     x = flat_start(prob) if x0 is None else np.array(x0, dtype=np.float64)
     res = []
     converged = False
@@ -222,4 +353,50 @@ def newton(prob: PowerFlowProblem, *, solver="rf", tol: float = 1e-10, maxiter: 
     if sensitivities and converged:
         lin.refactor(jacobian_values(prob, x))
         out.sensitivities = -lin.solve(control_jacobian(prob, x))
+    return out
+
+
+def _newton_device(prob, lin, tol, maxiter, x0, sensitivities, line_search) -> NewtonResult:
+    """The loop of newton() with x, F, Gx, Gu and the step on the device (DeviceAssembly), the
+    same steps and line search: only max |F| comes to the host per evaluation."""
+    import torch
+
+    asm = DeviceAssembly(prob, lin.A)
+    dev = lin.A.nzVal.device
+    x = torch.tensor(flat_start(prob) if x0 is None else np.asarray(x0, dtype=np.float64),
+                     dtype=torch.float64, device=dev)
+    if x.shape != (asm.n,):
+        raise ValueError(f"x0 has {x.shape[0]} entries, the problem {asm.n} unknowns")
+    xt, F, Ft, d = (torch.empty_like(x) for _ in range(4))
+    nrm = asm.mismatch(x, F)
+    res = []
+    converged = False
+    it = 0
+    for it in range(maxiter + 1):
+        res.append(nrm)
+        if nrm <= tol:
+            converged = True
+            break
+        if it == maxiter:
+            break
+        asm.jacobian(x)
+        lin.refactor_device()
+        d = lin.solve_device(F, d)            # Gx^{-1} F; the Newton step is -d
+        a = 1.0
+        while True:
+            nt = asm.mismatch(x, Ft, dx=d, alpha=-a, x_out=xt)
+            if not (line_search and a > 2.0 ** -12 and nt >= nrm):
+                break
+            a *= 0.5
+        x, xt = xt, x
+        F, Ft = Ft, F
+        nrm = nt
+    xh = x.cpu().numpy()
+    vm, va = state_to_voltages(prob, xh)
+    out = NewtonResult(xh, vm, va, it, converged, res)
+    if sensitivities and converged:
+        Gu = torch.empty((asm.n_ctrl, asm.n), dtype=torch.float64, device=dev).t()   # column-major
+        asm.jacobian(x, Gu)
+        lin.refactor_device()
+        out.sensitivities = -lin.solve_device(Gu).cpu().numpy()
     return out

@@ -143,7 +143,8 @@ typedef enum {
     BPF_KC_BACKSUB = 8, /* block back substitution of block-GMRES     */
     BPF_KC_MLP = 9,     /* learned warm start: tensor-core GEMMs       */
     BPF_KC_BATCH = 10,  /* batched solve: factor + persistent solve graph */
-    BPF_KC_COUNT = 11
+    BPF_KC_PF = 11,     /* power-flow mismatch and Jacobian assembly  */
+    BPF_KC_COUNT = 12
 } bpf_kernel_class;
 BPF_API bpf_status bpf_ctx_set_timing(bpf_ctx *ctx, int on);
 /* Totals since bpf_ctx_set_timing(ctx, 1): device milliseconds, launches, and the launches'
@@ -346,6 +347,35 @@ BPF_API bpf_status bpf_batch_unit_cycles(const bpf_batch *batch, long long *cycl
 BPF_API bpf_status bpf_batch_info(const bpf_batch *batch, int *nunits, int *grid,
                                   long long *device_bytes);
 BPF_API bpf_status bpf_batch_destroy(bpf_batch *batch);
+
+/* ---- power-flow assembly (the caller of the solve path) --------------------------------
+ * The Newton power-flow loop whose linear systems the path solves: the mismatch
+ * F(x) = S(V(x)) - S_spec, S = V conj(Ybus V), the Jacobian Gx = dF/dx on a fixed pattern and the
+ * control Jacobian Gu = dF/du, assembled on the device.  The reference's benchmark reads Gx and Gu
+ * that ExaPF assembled (benchmarks/benchmarks_nvidia.jl:29-39) and refactors Gx once per Newton
+ * step (src/cusolverRF.jl:304-314).  Unknowns x = [theta(non-slack buses); |V|(PQ buses)] and
+ * equations F = [P(non-slack); Q(PQ)], both in bus order; controls u = |V| of the slack bus, then
+ * of the PV buses in bus order (Gu: n x n_ctrl). */
+typedef struct bpf_pf bpf_pf;
+/* Ybus: HOST CSR, 0-based, n_bus rows, sorted unique columns, vals interleaved (re, im).
+ * bus_type: 1 PQ, 2 PV, 3 slack (exactly one).  vm_fixed / va_fixed (n_bus): |V| and angle at
+ * the buses where they are not unknowns; s_spec: 2 n_bus doubles (P, Q) interleaved.  jac: the
+ * device pattern of Gx (0- or 1-based); every entry the buses' coupling produces must be in it
+ * (BPF_ERR_INVALID_VALUE names the first missing one), other entries are written as zeros. */
+BPF_API bpf_status bpf_pf_create(bpf_ctx *ctx, int n_bus, const int *ybus_rowptr, const int *ybus_colind,
+                                 const double *ybus_vals, const int *bus_type, const double *vm_fixed,
+                                 const double *va_fixed, const double *s_spec, const bpf_csr_desc *jac,
+                                 bpf_pf **pf);
+BPF_API bpf_status bpf_pf_info(const bpf_pf *pf, int *n, int *n_ctrl, int *n_bus);
+/* F (device, n) = mismatch at x + alpha dx (dx nullable -> at x); x_out (nullable, may alias x)
+ * receives that point.  norm_inf (host, nullable): max |F|, NaN if any entry is; when given, the
+ * call synchronizes the context's stream. */
+BPF_API bpf_status bpf_pf_mismatch(bpf_pf *pf, const double *x, const double *dx, double alpha,
+                                   double *x_out, double *F, double *norm_inf);
+/* Gx values at x into jac_vals (device, the pattern's nnz, CSR order); gu (nullable, device,
+ * column-major n x n_ctrl, ld ldgu >= n) = Gu at x. */
+BPF_API bpf_status bpf_pf_jacobian(bpf_pf *pf, const double *x, double *jac_vals, double *gu, int ldgu);
+BPF_API bpf_status bpf_pf_destroy(bpf_pf *pf);
 
 /* ---- refactorization (cusolverRF replacement) ------------------------------------------ */
 /* CusolverRfLU(A; ordering, tol, fast_mode) / CusolverRfLUBatch(A, batch; ...):

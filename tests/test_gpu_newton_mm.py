@@ -46,6 +46,59 @@ def test_newton_on_the_device_matches_the_direct_loop(bpf, n_bus, solver):
     assert err <= tol, err
 
 
+@pytest.mark.parametrize("n_bus,seed", [(300, 3), (2000, 7)])
+def test_device_assembly_matches_the_numpy_assembly(bpf, n_bus, seed):
+    """bpf_pf_mismatch / bpf_pf_jacobian against mismatch(), jacobian_values(), control_jacobian()
+    (1e-12 relative: the same formulas, FMA-contracted complex products); the trial point
+    x + alpha dx bit for bit; max |F| equal to the largest |F| entry."""
+    import torch
+
+    prob = NT.make_problem(G.make_grid(n_bus, seed=seed))
+    A = bpf.CuSparseMatrixCSR.from_scipy(prob.pattern)
+    asm = NT.DeviceAssembly(prob, A)
+    assert (asm.n, asm.n_ctrl) == (prob.pattern.shape[0], len(prob.ctrl))
+    x = NT.perturbed_start(prob, 0.05, seed=seed)
+    dx = np.random.default_rng(seed).standard_normal(len(x))
+    xd, dxd = (torch.tensor(v, device="cuda") for v in (x, dx))
+    F, xt = torch.empty_like(xd), torch.empty_like(xd)
+    nrm = asm.mismatch(xd, F)
+    F0 = NT.mismatch(prob, x)
+    assert np.abs(F.cpu().numpy() - F0).max() <= 1e-12 * np.abs(F0).max()
+    assert nrm == float(F.abs().max())
+    nrm2 = asm.mismatch(xd, F, dx=dxd, alpha=-0.25, x_out=xt)
+    x2 = x + (-0.25) * dx
+    assert np.array_equal(xt.cpu().numpy(), x2)
+    F2 = NT.mismatch(prob, x2)
+    assert np.abs(F.cpu().numpy() - F2).max() <= 1e-12 * np.abs(F2).max()
+    assert nrm2 == float(F.abs().max())
+    Gu = torch.full((asm.n_ctrl, asm.n), 7.0, dtype=torch.float64, device="cuda").t()
+    A.nzVal.fill_(7.0)
+    asm.jacobian(xd, Gu)
+    J0 = NT.jacobian_values(prob, x)
+    assert np.abs(A.nzVal.cpu().numpy() - J0).max() <= 1e-12 * np.abs(J0).max()
+    Gu0 = NT.control_jacobian(prob, x)
+    assert np.abs(Gu.cpu().numpy() - Gu0).max() <= 1e-12 * np.abs(Gu0).max()
+    xd[3] = float("nan")
+    assert np.isnan(asm.mismatch(xd, F))
+
+
+def test_device_assembly_rejects_a_pattern_it_cannot_fill(bpf):
+    from blockpowerflow_b200 import _lib
+
+    prob = NT.make_problem(G.make_grid(300, seed=3))
+    P = prob.pattern.tolil()
+    r = 5
+    c = [j for j in P.rows[r] if j != r][0]
+    P[r, c] = 0
+    P = P.tocsr()
+    P.eliminate_zeros()
+    with pytest.raises(_lib.BPFError, match="lacks entry"):
+        NT.DeviceAssembly(prob, bpf.CuSparseMatrixCSR.from_scipy(P))
+    small = sp.csr_matrix(prob.pattern[:-1, :-1])
+    with pytest.raises(_lib.DimensionMismatch):
+        NT.DeviceAssembly(prob, bpf.CuSparseMatrixCSR.from_scipy(small))
+
+
 def test_dump_ingest_and_the_benchmark_solve(bpf, tmp_path):
     from blockpowerflow_b200 import mm
 
