@@ -220,11 +220,14 @@ class NewtonResult:
     sensitivities: np.ndarray | None = None   # dx/du = -Gx^{-1} Gu at the solution
 
 
-class _RFSolver:
+class RFSolver:
     """Linear solves of the loop on the cusolverRF-style refactorization: analysis once, then
-    refactor + solve per Newton step; the sensitivities reuse the last factorization."""
+    refactor + solve per Newton step; the sensitivities reuse the last factorization.  One
+    instance serves every power flow on the same pattern (pass it as newton(solver=...)): the
+    analysis is then paid once, as the reference's CusolverRfLU object is built once and
+    refactored per step (src/cusolverRF.jl:222,304-314)."""
 
-    def __init__(self, prob, nrhs, ordering):
+    def __init__(self, prob, nrhs=1, ordering="AMD"):
         import torch
 
         from . import cusolverrf as RF
@@ -260,10 +263,11 @@ class _RFSolver:
         return X
 
 
-class _GmresSolver:
-    """Linear solves of the loop by ILU(0)-preconditioned block-GMRES (refactor per step)."""
+class GmresSolver:
+    """Linear solves of the loop by ILU(0)-preconditioned block-GMRES (refactor per step); reusable
+    across power flows on the same pattern like RFSolver."""
 
-    def __init__(self, prob, nrhs, ordering, rtol=1e-12):
+    def __init__(self, prob, nrhs=1, ordering="AMD", rtol=1e-12):
         import torch
 
         from . import precond
@@ -314,7 +318,8 @@ def newton(prob: PowerFlowProblem, *, solver="rf", tol: float = 1e-10, maxiter: 
     with line_search, a step is halved (down to 2^-12) until ||F||_inf decreases.
 
     solver: "rf" (refactor + direct solve per step on the device, the reference's per-Newton-
-    step use of CusolverRfLU), "gmres" (ILU(0) refactor + block-GMRES), or an object with
+    step use of CusolverRfLU), "gmres" (ILU(0) refactor + block-GMRES), an RFSolver /
+    GmresSolver built earlier for this pattern (its analysis reused), or an object with
     refactor(values) and solve(B) methods (a host stand-in: then F, Gx and Gu are assembled by
     numpy).  With "rf" / "gmres" the mismatch, Gx and Gu are assembled on the device
     (DeviceAssembly) and x, F and the steps stay there.  With sensitivities=True, dx/du =
@@ -322,9 +327,9 @@ def newton(prob: PowerFlowProblem, *, solver="rf", tol: float = 1e-10, maxiter: 
     n_ctrl = len(prob.ctrl)
     nrhs = n_ctrl if sensitivities else 1
     if solver == "rf":
-        lin = _RFSolver(prob, nrhs, ordering)
+        lin = RFSolver(prob, nrhs, ordering)
     elif solver == "gmres":
-        lin = _GmresSolver(prob, nrhs, ordering)
+        lin = GmresSolver(prob, nrhs, ordering)
     else:
         lin = solver
     if hasattr(lin, "solve_device"):

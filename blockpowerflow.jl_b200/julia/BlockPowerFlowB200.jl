@@ -10,10 +10,12 @@ module BlockPowerFlowB200
 using LinearAlgebra
 using CUDA
 using CUDA.CUSPARSE
+using SparseArrays
 
 import LinearAlgebra: ldiv!
 
 export block_gmres, block_bicgstab, ilu0, ic0, CUSOLVERRF, BatchPlan, batch_solve!, BlockJacobiPreconditioner
+export PowerFlowAssembly, mismatch!, jacobian!
 
 const libbpf = joinpath(@__DIR__, "..", "lib", "libbpf.so")
 
@@ -270,6 +272,60 @@ function batch_solve!(Xs::Vector{CuMatrix{Float64}}, P::BatchPlan, Bs::Vector{Cu
                 [pointer(X) for X in Xs], Cint[stride(X, 2) for X in Xs], buf))
     stats = [unsafe_load(Ptr{CStats}(pointer(buf)) + (s - 1) * sizeof(CStats)) for s in 1:ns]
     return [(niter=Int(c.niter), solved=c.solved != 0, status=status_string(c.status)) for c in stats]
+end
+
+# ---- power-flow assembly (an addition: the Newton loop's F, Gx, Gu on the device) -------
+# Unknowns x = [theta(non-slack); |V|(PQ)], equations [P(non-slack); Q(PQ)], controls |V| of the
+# slack then the PV buses, all in bus order; bus_type: 1 PQ, 2 PV, 3 slack (exactly one).
+mutable struct PowerFlowAssembly
+    h::Ptr{Cvoid}
+    Gx::CuSparseMatrixCSR{Float64,Cint}
+    n::Int
+    nctrl::Int
+end
+
+function PowerFlowAssembly(Ybus::SparseMatrixCSC{ComplexF64}, bus_type::Vector{<:Integer},
+                           vm::Vector{Float64}, va::Vector{Float64}, Sspec::Vector{ComplexF64},
+                           Gx::CuSparseMatrixCSR{Float64,Cint})
+    nb = size(Ybus, 1)
+    Yt = SparseMatrixCSC(transpose(Ybus))          # CSC of the transpose = CSR of Ybus
+    rowptr = Cint.(Yt.colptr .- 1)
+    colind = Cint.(Yt.rowval .- 1)
+    vals = reinterpret(Float64, Yt.nzval) |> collect   # (re, im) interleaved
+    s = reinterpret(Float64, Sspec) |> collect
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:bpf_pf_create, libbpf), Cint,
+                (Ptr{Cvoid}, Cint, Ptr{Cint}, Ptr{Cint}, Ptr{Cdouble}, Ptr{Cint}, Ptr{Cdouble},
+                 Ptr{Cdouble}, Ptr{Cdouble}, Ref{CsrDesc}, Ref{Ptr{Cvoid}}),
+                ctx(), nb, rowptr, colind, vals, Cint.(bus_type), vm, va, s, Ref(desc(Gx)), r))
+    n, nc = Ref{Cint}(0), Ref{Cint}(0)
+    check(ccall((:bpf_pf_info, libbpf), Cint, (Ptr{Cvoid}, Ref{Cint}, Ref{Cint}, Ptr{Cint}),
+                r[], n, nc, C_NULL))
+    PF = PowerFlowAssembly(r[], Gx, n[], nc[])
+    finalizer(p -> ccall((:bpf_pf_destroy, libbpf), Cint, (Ptr{Cvoid},), p.h), PF)
+    return PF
+end
+
+# F = F(x + alpha dx) (dx nothing -> at x); xout (optional, may be x) receives that point.
+function mismatch!(F::CuVector{Float64}, PF::PowerFlowAssembly, x::CuVector{Float64},
+                   dx::Union{Nothing,CuVector{Float64}}=nothing, alpha::Float64=0.0,
+                   xout::Union{Nothing,CuVector{Float64}}=nothing)
+    length(x) == length(F) == PF.n || throw(DimensionMismatch("x and F need $(PF.n) entries"))
+    nrm = Ref{Cdouble}(0.0)
+    check(ccall((:bpf_pf_mismatch, libbpf), Cint,
+                (Ptr{Cvoid}, CuPtr{Cdouble}, CuPtr{Cdouble}, Cdouble, CuPtr{Cdouble}, CuPtr{Cdouble}, Ref{Cdouble}),
+                PF.h, pointer(x), dx === nothing ? CU_NULL : pointer(dx), alpha,
+                xout === nothing ? CU_NULL : pointer(xout), pointer(F), nrm))
+    return nrm[]
+end
+
+# Gx values at x into PF.Gx (refactor it next); Gu (n x nctrl), if given, = dF/du.
+function jacobian!(PF::PowerFlowAssembly, x::CuVector{Float64}, Gu::Union{Nothing,CuMatrix{Float64}}=nothing)
+    Gu === nothing || size(Gu) == (PF.n, PF.nctrl) || throw(DimensionMismatch("Gu must be $(PF.n) x $(PF.nctrl)"))
+    check(ccall((:bpf_pf_jacobian, libbpf), Cint, (Ptr{Cvoid}, CuPtr{Cdouble}, CuPtr{Cdouble}, CuPtr{Cdouble}, Cint),
+                PF.h, pointer(x), pointer(nonzeros(PF.Gx)), Gu === nothing ? CU_NULL : pointer(Gu),
+                Gu === nothing ? 0 : stride(Gu, 2)))
+    return PF.Gx
 end
 
 # ---- block-BiCGSTAB (src/block_bicgstab.jl:182-299) -----------------------------------

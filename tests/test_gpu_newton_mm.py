@@ -99,6 +99,20 @@ def test_device_assembly_rejects_a_pattern_it_cannot_fill(bpf):
         NT.DeviceAssembly(prob, bpf.CuSparseMatrixCSR.from_scipy(small))
 
 
+def test_a_reused_solver_serves_a_second_power_flow(bpf):
+    """One RFSolver (one analysis) for two power flows on the same pattern: the second solve
+    repeats the first (the refactorization starts from fresh values every step)."""
+    prob = NT.make_problem(G.make_grid(300, seed=7))
+    x0 = NT.perturbed_start(prob, 0.01, seed=2)
+    lin = NT.RFSolver(prob, len(prob.ctrl))
+    r1 = NT.newton(prob, solver=lin, x0=x0, tol=1e-10, sensitivities=True)
+    r2 = NT.newton(prob, solver=lin, x0=x0, tol=1e-10, sensitivities=True)
+    assert r1.converged and r2.converged and r1.iterations == r2.iterations
+    np.testing.assert_allclose(r2.x, r1.x, rtol=0, atol=1e-12)
+    err = np.linalg.norm(r2.sensitivities - r1.sensitivities) / np.linalg.norm(r1.sensitivities)
+    assert err <= 1e-12, err
+
+
 def test_dump_ingest_and_the_benchmark_solve(bpf, tmp_path):
     from blockpowerflow_b200 import mm
 
