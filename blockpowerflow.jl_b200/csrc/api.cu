@@ -153,13 +153,16 @@ bpf_status prec_setup(bpf_ctx *ctx, int kind, int n, const std::vector<int> &rp,
     TriHost up = ic ? build_tri(n, rp.data(), ci.data(), diag.data(), 2, false)
                     : build_tri(n, rp.data(), ci.data(), diag.data(), 1, false);
     std::vector<int> pp, pdst, psrc;
-    build_pairs(n, rp.data(), ci.data(), diag.data(), ic, pp, pdst, psrc);
+    const bool pairs_ok = build_pairs(n, rp.data(), ci.data(), diag.data(), ic, pp, pdst, psrc);
     P->npairs = (long long)pdst.size();
     auto fail = [&](bpf_status s) {
         cudaStreamSynchronize(ctx->stream);
         bpf_prec_destroy(P);
         return s;
     };
+    if (!pairs_ok)
+        return fail(set_error(ctx, BPF_ERR_NOT_SUPPORTED,
+                              "factorization update pairs exceed 2^31 - 1 (pattern of %d entries too dense)", nnz));
     bpf_status s;
     if ((s = tri_upload(ctx, lo, P->lower)) != BPF_SUCCESS) return fail(s);
     if ((s = tri_upload(ctx, up, P->upper)) != BPF_SUCCESS) return fail(s);

@@ -1168,7 +1168,8 @@ bpf_status bpf_batch_plan(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A, const i
         if (bad >= 0)
             return fail(set_error(ctx, BPF_ERR_SINGULAR, "batch: system %d: structurally zero diagonal at row %d", s, bad));
         std::vector<int> pp, pdst, psrc;
-        build_pairs(n, rp.data(), ci.data(), diag.data(), false, pp, pdst, psrc);
+        if (!build_pairs(n, rp.data(), ci.data(), diag.data(), false, pp, pdst, psrc))
+            return fail(set_error(ctx, BPF_ERR_NOT_SUPPORTED, "batch: system %d: ILU(0) update pairs exceed 2^31 - 1", s));
         TriHost L = build_tri(n, rp.data(), ci.data(), diag.data(), 0, true);
         TriHost U = build_tri(n, rp.data(), ci.data(), diag.data(), 1, false);
         Offs &f = offs[s];

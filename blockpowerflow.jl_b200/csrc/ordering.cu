@@ -2,6 +2,7 @@
 // by the cusolverRF-style analysis (src/cusolverRF.jl:70-95, where cusolverSp computes the
 // :AMD / :MDQ / :RCM orderings) and the reordered ILU(0) / IC(0) preconditioners.
 #include <algorithm>
+#include <functional>
 #include <iterator>
 #include <set>
 #include <vector>
@@ -30,36 +31,60 @@ void sym_adjacency(int n, const std::vector<int> &rp, const std::vector<int> &ci
 }
 
 // Minimum degree on the explicit elimination graph: eliminate a node of least current
-// degree (smallest index on ties), turning its neighbourhood into a clique.
+// degree (smallest index on ties), turning its neighbourhood into a clique.  The queue is a
+// binary heap of (degree, node) with lazy deletion (an entry whose degree is no longer the
+// node's is skipped when it surfaces), so the node taken is the smallest current (degree,
+// node) pair; the clique is formed with a marker array on unsorted adjacency lists.
 std::vector<int> order_min_degree(int n, const std::vector<int> &rp, const std::vector<int> &ci) {
     std::vector<std::vector<int>> adj;
     sym_adjacency(n, rp, ci, adj);
-    std::set<std::pair<int, int>> pq;
+    using Key = std::pair<int, int>;
+    std::vector<Key> heap;
+    heap.reserve(2 * (size_t)n);
     std::vector<int> deg(n);
     for (int v = 0; v < n; v++) {
         deg[v] = (int)adj[v].size();
-        pq.insert({deg[v], v});
+        heap.push_back({deg[v], v});
     }
-    std::vector<int> order;
+    std::make_heap(heap.begin(), heap.end(), std::greater<Key>());
+    std::vector<char> gone(n, 0);
+    std::vector<int> mark(n, -1), order, nb;
     order.reserve(n);
-    std::vector<int> merged;
-    while (!pq.empty()) {
-        const int v = pq.begin()->second;
-        pq.erase(pq.begin());
+    int stamp = 0;
+    while (!heap.empty()) {
+        std::pop_heap(heap.begin(), heap.end(), std::greater<Key>());
+        const Key t = heap.back();
+        heap.pop_back();
+        const int v = t.second;
+        if (gone[v] || t.first != deg[v]) continue;
+        gone[v] = 1;
         order.push_back(v);
-        const std::vector<int> nb = adj[v];
+        nb.swap(adj[v]);
         for (int u : nb) {
-            merged.clear();
-            std::set_union(adj[u].begin(), adj[u].end(), nb.begin(), nb.end(), std::back_inserter(merged));
-            merged.erase(std::remove_if(merged.begin(), merged.end(), [&](int w) { return w == u || w == v; }),
-                         merged.end());
-            pq.erase({deg[u], u});
-            adj[u].swap(merged);
-            deg[u] = (int)adj[u].size();
-            pq.insert({deg[u], u});
+            // adj[u] <- adj[u] U nb \ {u, v}
+            std::vector<int> &a = adj[u];
+            const int s = stamp++;
+            size_t w = 0;
+            for (size_t r = 0; r < a.size(); r++) {
+                const int x = a[r];
+                if (x == v) continue;
+                mark[x] = s;
+                a[w++] = x;
+            }
+            a.resize(w);
+            mark[u] = s;
+            for (int x : nb)
+                if (mark[x] != s) {
+                    mark[x] = s;
+                    a.push_back(x);
+                }
+            if ((int)a.size() != deg[u]) {
+                deg[u] = (int)a.size();
+                heap.push_back({deg[u], u});
+                std::push_heap(heap.begin(), heap.end(), std::greater<Key>());
+            }
         }
-        adj[v].clear();
-        adj[v].shrink_to_fit();
+        std::vector<int>().swap(nb);
     }
     return order;
 }

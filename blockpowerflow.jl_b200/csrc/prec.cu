@@ -18,6 +18,7 @@
 //  * FP32 factors (factor_dtype = BPF_F32) keep float copies of L, U and 1/diag, read half the
 //    factor bytes and compute in FP32; the block stays FP64 in memory.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <numeric>
 
@@ -127,40 +128,68 @@ TriHost build_tri(int n, const int *rp, const int *ci, const int *diag, int part
 // the pattern gives (dst = pos(i,j), src = pos(k,j)); applied as fv[dst] -= fv[e] * fv[src].
 // IC(0) pairs: for the L entry e = (i,k), every j < k with (i,j) and (k,j) in the lower
 // pattern gives (pos(i,j), pos(k,j)); fv[e] -= sum fv[pos(i,j)] * fv[pos(k,j)].
-void build_pairs(int n, const int *rp, const int *ci, const int *diag, bool ic,
+bool build_pairs(int n, const int *rp, const int *ci, const int *diag, bool ic,
                  std::vector<int> &pp, std::vector<int> &pdst, std::vector<int> &psrc) {
-    int nnz = rp[n];
+    const int nnz = rp[n];
     pp.assign(nnz + 1, 0);
-    pdst.clear();
-    psrc.clear();
     std::vector<int> pos(n, -1);
-    for (int i = 0; i < n; i++) {
-        for (int k = rp[i]; k < rp[i + 1]; k++) pos[ci[k]] = k;
-        for (int e = rp[i]; e < rp[i + 1]; e++) {
-            pp[e] = (int)pdst.size();
-            int kc = ci[e];
-            if (kc >= i) continue;
-            if (!ic) {
-                for (int j = diag[kc] + 1; j < rp[kc + 1]; j++) {
-                    int q = pos[ci[j]];
-                    if (q >= 0) {
-                        pdst.push_back(q);
-                        psrc.push_back(j);
+    // two passes over the same visit order: count the pairs of every entry, then fill arrays of
+    // the exact size (tens of millions of pairs for a full LU pattern)
+    for (int pass = 0; pass < 2; pass++) {
+        int *dst = pass ? pdst.data() : nullptr, *src = pass ? psrc.data() : nullptr;
+        long long cnt = 0;
+        for (int i = 0; i < n; i++) {
+            for (int k = rp[i]; k < rp[i + 1]; k++) pos[ci[k]] = k;
+            for (int e = rp[i]; e < rp[i + 1]; e++) {
+                if (pass) cnt = pp[e];
+                const int kc = ci[e];
+                long long c = 0;
+                if (kc < i) {
+                    if (!ic) {
+                        for (int j = diag[kc] + 1; j < rp[kc + 1]; j++) {
+                            const int q = pos[ci[j]];
+                            if (q >= 0) {
+                                if (pass) {
+                                    dst[cnt + c] = q;
+                                    src[cnt + c] = j;
+                                }
+                                c++;
+                            }
+                        }
+                    } else {
+                        for (int j = rp[kc]; j < diag[kc]; j++) {
+                            const int q = pos[ci[j]];
+                            if (q >= 0 && ci[j] < kc) {
+                                if (pass) {
+                                    dst[cnt + c] = q;
+                                    src[cnt + c] = j;
+                                }
+                                c++;
+                            }
+                        }
                     }
                 }
-            } else {
-                for (int j = rp[kc]; j < diag[kc]; j++) {
-                    int q = pos[ci[j]];
-                    if (q >= 0 && ci[j] < kc) {
-                        pdst.push_back(q);
-                        psrc.push_back(j);
-                    }
-                }
+                if (!pass) pp[e + 1] = (int)c;
             }
+            for (int k = rp[i]; k < rp[i + 1]; k++) pos[ci[k]] = -1;
         }
-        for (int k = rp[i]; k < rp[i + 1]; k++) pos[ci[k]] = -1;
+        if (!pass) {
+            long long total = 0;
+            for (int e = 0; e < nnz; e++) {
+                total += pp[e + 1];
+                if (total > INT_MAX) {   // offsets are int: the caller reports the pattern as too dense
+                    pp.clear();
+                    pdst.clear();
+                    psrc.clear();
+                    return false;
+                }
+                pp[e + 1] = (int)total;
+            }
+            pdst.resize(pp[nnz]);
+            psrc.resize(pp[nnz]);
+        }
     }
-    pp[nnz] = (int)pdst.size();
+    return true;
 }
 
 // ------------------------------------------------------------------------------------

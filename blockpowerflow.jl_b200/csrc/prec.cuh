@@ -64,7 +64,8 @@ struct TriDev {
 enum PrecKind { PREC_ILU0 = 1, PREC_IC0 = 2, PREC_LU = 3, PREC_BJ = 4 };
 
 TriHost build_tri(int n, const int *rp, const int *ci, const int *diag, int part, bool unit);
-void build_pairs(int n, const int *rp, const int *ci, const int *diag, bool ic,
+// false (and empty outputs) when the pair count exceeds INT_MAX
+bool build_pairs(int n, const int *rp, const int *ci, const int *diag, bool ic,
                  std::vector<int> &pp, std::vector<int> &pdst, std::vector<int> &psrc);
 bpf_status tri_upload(bpf_ctx *ctx, const TriHost &h, TriDev &d);
 void tri_free(TriDev &d);
