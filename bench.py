@@ -462,16 +462,27 @@ def config_newton9k(args):
     x0 = NT.perturbed_start(prob, 0.001, seed=1)
     NT.newton(prob, solver="rf", x0=x0, tol=1e-10, sensitivities=True)   # warm-up (analysis, JIT)
     torch.cuda.synchronize()
-    bpf._lib.set_timing(True)
-    t0 = time.time()
-    r = NT.newton(prob, solver="rf", x0=x0, tol=1e-10, sensitivities=True)
-    torch.cuda.synchronize()
-    t_gpu = time.time() - t0
-    kern = _class_rates(bpf, ("factor", "trsv", "pf"))
+    # three cold solves (each with its own RF analysis); the median is reported, since their host
+    # part (analysis, the 136 MB sensitivity block's copy to the host) meets the shared host's
+    # load; kernel times are taken from the first
+    cold = []
+    for rep in range(3):
+        bpf._lib.set_timing(rep == 0)
+        t0 = time.time()
+        r = NT.newton(prob, solver="rf", x0=x0, tol=1e-10, sensitivities=True)
+        torch.cuda.synchronize()
+        cold.append(time.time() - t0)
+        if rep == 0:
+            kern = _class_rates(bpf, ("factor", "trsv", "pf"))
     bpf._lib.set_timing(False)
+    t_gpu = float(np.median(cold))
     # the same power flow with the solver (its RF analysis) built once for the pattern and reused,
     # as a sequence of power flows on one network would run
+    torch.cuda.synchronize()
+    t0 = time.time()
     lin = NT.RFSolver(prob, len(prob.ctrl), "AMD")
+    torch.cuda.synchronize()
+    t_analysis = time.time() - t0
     NT.newton(prob, solver=lin, x0=x0, tol=1e-10, sensitivities=True)
     torch.cuda.synchronize()
     t0 = time.time()
@@ -498,10 +509,11 @@ def config_newton9k(args):
                        "tol": 1e-10},
             "metric": "Newton power flow + sensitivities, seconds", "unit": "s", "higher_is_better": False,
             "value": t_gpu, "iterations": r.iterations, "converged": bool(r.converged),
+            "cold_samples_s": cold, "rf_analysis_s": t_analysis,
             "analysis_reused": {"value": t_reuse, "unit": "s", "iterations": rw.iterations,
                                 "converged": bool(rw.converged)},
             "residuals": r.residuals, "device_linear_ms": dev_ms, "device_assembly_ms": asm_ms, "kernels": kern,
-            "host_ms": 1e3 * t_gpu - dev_ms - asm_ms,
+            "host_ms": 1e3 * cold[0] - dev_ms - asm_ms,
             "sensitivity_rel_diff_vs_superlu": float(np.linalg.norm(r.sensitivities - rc.sensitivities)
                                                      / np.linalg.norm(rc.sensitivities)),
             "cpu_baseline": {"value": t_cpu, "unit": "s", "cores": 1,

@@ -403,5 +403,7 @@ def _newton_device(prob, lin, tol, maxiter, x0, sensitivities, line_search) -> N
         Gu = torch.empty((asm.n_ctrl, asm.n), dtype=torch.float64, device=dev).t()   # column-major
         asm.jacobian(x, Gu)
         lin.refactor_device()
-        out.sensitivities = -lin.solve_device(Gu).cpu().numpy()
+        S = lin.solve_device(Gu).cpu().numpy()
+        np.negative(S, out=S)                 # in place: one n x n_ctrl host block, not two
+        out.sensitivities = S
     return out
