@@ -355,7 +355,8 @@ BPF_API bpf_status bpf_batch_destroy(bpf_batch *batch);
  * that ExaPF assembled (benchmarks/benchmarks_nvidia.jl:29-39) and refactors Gx once per Newton
  * step (src/cusolverRF.jl:304-314).  Unknowns x = [theta(non-slack buses); |V|(PQ buses)] and
  * equations F = [P(non-slack); Q(PQ)], both in bus order; controls u = |V| of the slack bus, then
- * of the PV buses in bus order (Gu: n x n_ctrl). */
+ * of the PV buses in bus order (Gu: n x n_ctrl).  An object holds the bus voltages of its last
+ * evaluation and its norm word: one call at a time per object (its context's stream orders them). */
 typedef struct bpf_pf bpf_pf;
 /* Ybus: HOST CSR, 0-based, n_bus rows, sorted unique columns, vals interleaved (re, im).
  * bus_type: 1 PQ, 2 PV, 3 slack (exactly one).  vm_fixed / va_fixed (n_bus): |V| and angle at
