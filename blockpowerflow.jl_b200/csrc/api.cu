@@ -152,7 +152,8 @@ bpf_status prec_setup(bpf_ctx *ctx, int kind, int n, const std::vector<int> &rp,
     TriHost lo = build_tri(n, rp.data(), ci.data(), diag.data(), 0, !ic);
     TriHost up = ic ? build_tri(n, rp.data(), ci.data(), diag.data(), 2, false)
                     : build_tri(n, rp.data(), ci.data(), diag.data(), 1, false);
-    std::vector<int> pp, pdst, psrc;
+    std::vector<int> pp;
+    PairVec pdst, psrc;
     const bool pairs_ok = build_pairs(n, rp.data(), ci.data(), diag.data(), ic, pp, pdst, psrc);
     P->npairs = (long long)pdst.size();
     auto fail = [&](bpf_status s) {
@@ -167,7 +168,7 @@ bpf_status prec_setup(bpf_ctx *ctx, int kind, int n, const std::vector<int> &rp,
     if ((s = tri_upload(ctx, lo, P->lower)) != BPF_SUCCESS) return fail(s);
     if ((s = tri_upload(ctx, up, P->upper)) != BPF_SUCCESS) return fail(s);
     cudaError_t e = cudaSuccess;
-    auto up_i = [&](int **d, const std::vector<int> &h) {
+    auto up_i = [&](int **d, const auto &h) {   // std::vector<int> or PairVec
         if (e != cudaSuccess || h.empty()) return;
         e = cudaMalloc((void **)d, sizeof(int) * h.size());
         if (e == cudaSuccess)

@@ -1065,8 +1065,8 @@ struct Packer {
         if (bytes && src) memcpy(host.data() + off, src, bytes);
         return off;
     }
-    template <typename T>
-    size_t add(const std::vector<T> &v) { return add(v.data(), v.size() * sizeof(T)); }
+    template <typename T, typename A>
+    size_t add(const std::vector<T, A> &v) { return add(v.data(), v.size() * sizeof(T)); }
     size_t reserve(size_t bytes) { return add(nullptr, bytes); }
 };
 
@@ -1167,7 +1167,8 @@ bpf_status bpf_batch_plan(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A, const i
         const int bad = permute_pattern(n, arp, aci, perm, rp, ci, amap, diag);
         if (bad >= 0)
             return fail(set_error(ctx, BPF_ERR_SINGULAR, "batch: system %d: structurally zero diagonal at row %d", s, bad));
-        std::vector<int> pp, pdst, psrc;
+        std::vector<int> pp;
+        PairVec pdst, psrc;
         if (!build_pairs(n, rp.data(), ci.data(), diag.data(), false, pp, pdst, psrc))
             return fail(set_error(ctx, BPF_ERR_NOT_SUPPORTED, "batch: system %d: ILU(0) update pairs exceed 2^31 - 1", s));
         TriHost L = build_tri(n, rp.data(), ci.data(), diag.data(), 0, true);

@@ -18,9 +18,11 @@
 //  * FP32 factors (factor_dtype = BPF_F32) keep float copies of L, U and 1/diag, read half the
 //    factor bytes and compute in FP32; the block stays FP64 in memory.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <numeric>
+#include <thread>
 
 #include "bpf_internal.cuh"
 #include "prec.cuh"
@@ -129,20 +131,19 @@ TriHost build_tri(int n, const int *rp, const int *ci, const int *diag, int part
 // IC(0) pairs: for the L entry e = (i,k), every j < k with (i,j) and (k,j) in the lower
 // pattern gives (pos(i,j), pos(k,j)); fv[e] -= sum fv[pos(i,j)] * fv[pos(k,j)].
 bool build_pairs(int n, const int *rp, const int *ci, const int *diag, bool ic,
-                 std::vector<int> &pp, std::vector<int> &pdst, std::vector<int> &psrc) {
+                 std::vector<int> &pp, PairVec &pdst, PairVec &psrc) {
     const int nnz = rp[n];
     pp.assign(nnz + 1, 0);
-    std::vector<int> pos(n, -1);
-    // two passes over the same visit order: count the pairs of every entry, then fill arrays of
-    // the exact size (tens of millions of pairs for a full LU pattern)
-    for (int pass = 0; pass < 2; pass++) {
+    // rows [i0, i1): pass 0 counts the pairs of every entry into pp[e + 1]; pass 1 writes them at
+    // the entry's prefix offset pp[e].  Every entry belongs to one row, so rows can be taken by
+    // any thread in any order and the output is the same.
+    auto rows = [&](int pass, int i0, int i1, std::vector<int> &pos) {
         int *dst = pass ? pdst.data() : nullptr, *src = pass ? psrc.data() : nullptr;
-        long long cnt = 0;
-        for (int i = 0; i < n; i++) {
+        for (int i = i0; i < i1; i++) {
             for (int k = rp[i]; k < rp[i + 1]; k++) pos[ci[k]] = k;
             for (int e = rp[i]; e < rp[i + 1]; e++) {
-                if (pass) cnt = pp[e];
                 const int kc = ci[e];
+                const long long base = pass ? pp[e] : 0;
                 long long c = 0;
                 if (kc < i) {
                     if (!ic) {
@@ -150,8 +151,8 @@ bool build_pairs(int n, const int *rp, const int *ci, const int *diag, bool ic,
                             const int q = pos[ci[j]];
                             if (q >= 0) {
                                 if (pass) {
-                                    dst[cnt + c] = q;
-                                    src[cnt + c] = j;
+                                    dst[base + c] = q;
+                                    src[base + c] = j;
                                 }
                                 c++;
                             }
@@ -161,34 +162,58 @@ bool build_pairs(int n, const int *rp, const int *ci, const int *diag, bool ic,
                             const int q = pos[ci[j]];
                             if (q >= 0 && ci[j] < kc) {
                                 if (pass) {
-                                    dst[cnt + c] = q;
-                                    src[cnt + c] = j;
+                                    dst[base + c] = q;
+                                    src[base + c] = j;
                                 }
                                 c++;
                             }
                         }
                     }
                 }
-                if (!pass) pp[e + 1] = (int)c;
+                if (!pass) pp[e + 1] = (int)std::min<long long>(c, INT_MAX);
             }
             for (int k = rp[i]; k < rp[i + 1]; k++) pos[ci[k]] = -1;
         }
-        if (!pass) {
-            long long total = 0;
-            for (int e = 0; e < nnz; e++) {
-                total += pp[e + 1];
-                if (total > INT_MAX) {   // offsets are int: the caller reports the pattern as too dense
-                    pp.clear();
-                    pdst.clear();
-                    psrc.clear();
-                    return false;
-                }
-                pp[e + 1] = (int)total;
-            }
-            pdst.resize(pp[nnz]);
-            psrc.resize(pp[nnz]);
+    };
+    // large patterns (the LU patterns of the refactorization) on several host threads, each with
+    // its own position array, taking blocks of 64 rows from a shared counter
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nthreads = nnz >= 200000 ? (int)std::min(16u, std::max(1u, hw)) : 1;
+    auto run = [&](int pass) {
+        if (nthreads <= 1) {
+            std::vector<int> pos(n, -1);
+            rows(pass, 0, n, pos);
+            return;
         }
+        std::atomic<int> next(0);
+        std::vector<std::thread> pool;
+        pool.reserve(nthreads);
+        for (int t = 0; t < nthreads; t++)
+            pool.emplace_back([&]() {
+                std::vector<int> pos(n, -1);
+                for (;;) {
+                    const int b = next.fetch_add(64);
+                    if (b >= n) break;
+                    rows(pass, b, std::min(n, b + 64), pos);
+                }
+            });
+        for (auto &th : pool) th.join();
+    };
+    run(0);
+    long long total = 0;
+    for (int e = 0; e < nnz; e++) {
+        total += pp[e + 1];
+        if (total > INT_MAX) {   // offsets are int: the caller reports the pattern as too dense
+            pp.clear();
+            pdst.clear();
+            psrc.clear();
+            return false;
+        }
+        pp[e + 1] = (int)total;
     }
+    pdst.resize(pp[nnz]);   // left uninitialised (NoInitAlloc): pass 1 writes every entry
+    psrc.resize(pp[nnz]);
+    run(1);
     return true;
 }
 

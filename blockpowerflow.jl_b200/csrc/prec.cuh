@@ -1,7 +1,9 @@
 // Internal types of the preconditioner / triangular-factor machinery.
 #pragma once
 
+#include <memory>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "bpf_internal.cuh"
@@ -64,9 +66,32 @@ struct TriDev {
 enum PrecKind { PREC_ILU0 = 1, PREC_IC0 = 2, PREC_LU = 3, PREC_BJ = 4 };
 
 TriHost build_tri(int n, const int *rp, const int *ci, const int *diag, int part, bool unit);
+// An allocator whose value-less construct leaves the element uninitialised, so resize() of a
+// buffer that is written in full right after (tens of millions of update pairs) neither zero-fills
+// it nor takes its first-touch page faults on one thread.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
+    template <typename U>
+    void construct(U *p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new (static_cast<void *>(p)) U;
+    }
+    template <typename U, typename... Args>
+    void construct(U *p, Args &&...args) {
+        ::new (static_cast<void *>(p)) U(std::forward<Args>(args)...);
+    }
+};
+using PairVec = std::vector<int, NoInitAlloc<int>>;
+
 // false (and empty outputs) when the pair count exceeds INT_MAX
 bool build_pairs(int n, const int *rp, const int *ci, const int *diag, bool ic,
-                 std::vector<int> &pp, std::vector<int> &pdst, std::vector<int> &psrc);
+                 std::vector<int> &pp, PairVec &pdst, PairVec &psrc);
 bpf_status tri_upload(bpf_ctx *ctx, const TriHost &h, TriDev &d);
 void tri_free(TriDev &d);
 bpf_status tri_scatter(bpf_ctx *ctx, const TriDev &d, const double *fv);
