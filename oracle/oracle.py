@@ -253,3 +253,77 @@ def block_jacobi_apply(A, order, block_size, X):
         Ab = A[rows][:, rows].toarray()
         Y[rows] = np.linalg.solve(Ab, X[rows])
     return Y
+
+
+def pf_assemble(ybus_rowptr, ybus_colind, ybus_vals, bus_type, vm_fixed, va_fixed, s_spec, x, pattern):
+    """Power-flow mismatch F, Jacobian Gx on `pattern` and control Jacobian Gu at the state x,
+    restated entry by entry from the host arguments of bpf_pf_create (the Newton loop around the
+    reference's solve path; ExaPF, which assembled the reference benchmark's Gx / Gu dumps
+    (benchmarks/benchmarks_nvidia.jl:29-39), is not part of the reference).
+
+    Polar form with S = V conj(I), I = Ybus V:
+      dS_i/dtheta_k = j V_i ([i == k] conj(I_i) - conj(Y_ik V_k)),
+      dS_i/d|V_k|   = V_i conj(Y_ik V_k / |V_k|) + [i == k] conj(I_i) V_i / |V_i|.
+    Unknowns: theta at every non-slack bus (bus order), then |V| at the PQ buses (bus order);
+    equations P, Q in the same order; controls: |V| of the slack bus, then of the PV buses.
+    Returns (F, Gx values in pattern's CSR order, Gu dense n x n_ctrl); raises ValueError if an
+    entry the coupling produces is missing from the pattern."""
+    rp = np.asarray(ybus_rowptr)
+    ci = np.asarray(ybus_colind)
+    yv = np.asarray(ybus_vals, dtype=np.float64)
+    bt = np.asarray(bus_type)
+    nb = len(bt)
+    slack = int(np.flatnonzero(bt == 3)[0])
+    ia = np.full(nb, -1)
+    ia[np.arange(nb) != slack] = np.arange(nb - 1)
+    pq = np.flatnonzero(bt == 1)
+    im = np.full(nb, -1)
+    im[pq] = nb - 1 + np.arange(len(pq))
+    ctrl_buses = np.concatenate([[slack], np.flatnonzero(bt == 2)])
+    ctrl = np.full(nb, -1)
+    ctrl[ctrl_buses] = np.arange(len(ctrl_buses))
+    n = (nb - 1) + len(pq)
+    x = np.asarray(x, dtype=np.float64)
+    va = np.where(ia >= 0, x[np.maximum(ia, 0)], va_fixed)
+    vm = np.where(im >= 0, x[np.maximum(im, 0)], vm_fixed)
+    V = vm * np.exp(1j * va)
+    y = yv[0::2] + 1j * yv[1::2]
+    rows = np.repeat(np.arange(nb), np.diff(rp))
+    # the I_i terms attach at the diagonal entry: every nonempty row must hold it (the library
+    # inserts a missing one; this restatement does not)
+    has_diag = np.zeros(nb, dtype=bool)
+    has_diag[rows[rows == ci]] = True
+    if np.any(~has_diag & (np.diff(rp) > 0)):
+        raise ValueError("a nonempty Ybus row lacks its diagonal entry")
+    t = y * V[ci]
+    I = np.bincount(rows, t.real, nb) + 1j * np.bincount(rows, t.imag, nb)
+    S = V * np.conj(I) - (np.asarray(s_spec)[0::2] + 1j * np.asarray(s_spec)[1::2])
+    F = np.zeros(n)
+    F[ia[ia >= 0]] = S.real[ia >= 0]
+    F[im[im >= 0]] = S.imag[im >= 0]
+    i, k = rows, ci
+    diag = i == k
+    dth = 1j * V[i] * (np.where(diag, np.conj(I[i]), 0) - np.conj(y * V[k]))
+    dm = V[i] * np.conj(y * V[k] / np.abs(V[k])) + np.where(diag, np.conj(I[i]) * V[i] / np.abs(V[i]), 0)
+    P = sp.csr_matrix(pattern)
+    if not P.has_sorted_indices:   # CSR order of the values, as the library requires it
+        raise ValueError("pattern columns must be sorted within each row")
+    gx = np.zeros(P.nnz)
+    for rr, cc, vv in ((ia[i], ia[k], dth.real), (ia[i], im[k], dm.real),
+                       (im[i], ia[k], dth.imag), (im[i], im[k], dm.imag)):
+        for r_, c_, v_ in zip(rr, cc, vv):
+            if r_ < 0 or c_ < 0:
+                continue
+            lo, hi = P.indptr[r_], P.indptr[r_ + 1]
+            pos = lo + np.searchsorted(P.indices[lo:hi], c_)
+            if pos >= hi or P.indices[pos] != c_:
+                if v_ == 0.0:
+                    continue
+                raise ValueError(f"pattern lacks entry ({r_}, {c_})")
+            gx[pos] = v_
+    Gu = np.zeros((n, len(ctrl_buses)))
+    sel = ctrl[k] >= 0
+    for rr, vv in ((ia[i], dm.real), (im[i], dm.imag)):
+        s2 = sel & (rr >= 0)
+        Gu[rr[s2], ctrl[k][s2]] = vv[s2]
+    return F, gx, Gu

@@ -49,9 +49,12 @@ def test_newton_on_the_device_matches_the_direct_loop(bpf, n_bus, solver):
 @pytest.mark.parametrize("n_bus,seed", [(300, 3), (2000, 7)])
 def test_device_assembly_matches_the_numpy_assembly(bpf, n_bus, seed):
     """bpf_pf_mismatch / bpf_pf_jacobian against mismatch(), jacobian_values(), control_jacobian()
-    (1e-12 relative: the same formulas, FMA-contracted complex products); the trial point
-    x + alpha dx bit for bit; max |F| equal to the largest |F| entry."""
+    (1e-12 relative: the same formulas, FMA-contracted complex products) and against the oracle's
+    entry-by-entry restatement over the same host arguments (1e-11); the trial point x + alpha dx
+    bit for bit; max |F| equal to the largest |F| entry."""
     import torch
+
+    import oracle as O
 
     prob = NT.make_problem(G.make_grid(n_bus, seed=seed))
     A = bpf.CuSparseMatrixCSR.from_scipy(prob.pattern)
@@ -64,6 +67,8 @@ def test_device_assembly_matches_the_numpy_assembly(bpf, n_bus, seed):
     nrm = asm.mismatch(xd, F)
     F0 = NT.mismatch(prob, x)
     assert np.abs(F.cpu().numpy() - F0).max() <= 1e-12 * np.abs(F0).max()
+    Fo, gxo, Guo = O.pf_assemble(*NT.bus_arrays(prob), x, prob.pattern)
+    assert np.abs(F.cpu().numpy() - Fo).max() <= 1e-11 * np.abs(Fo).max()
     assert nrm == float(F.abs().max())
     nrm2 = asm.mismatch(xd, F, dx=dxd, alpha=-0.25, x_out=xt)
     x2 = x + (-0.25) * dx
@@ -78,6 +83,8 @@ def test_device_assembly_matches_the_numpy_assembly(bpf, n_bus, seed):
     assert np.abs(A.nzVal.cpu().numpy() - J0).max() <= 1e-12 * np.abs(J0).max()
     Gu0 = NT.control_jacobian(prob, x)
     assert np.abs(Gu.cpu().numpy() - Gu0).max() <= 1e-12 * np.abs(Gu0).max()
+    assert np.abs(A.nzVal.cpu().numpy() - gxo).max() <= 1e-11 * np.abs(gxo).max()
+    assert np.abs(Gu.cpu().numpy() - Guo).max() <= 1e-11 * np.abs(Guo).max()
     xd[3] = float("nan")
     assert np.isnan(asm.mismatch(xd, F))
 
