@@ -16,6 +16,7 @@ import LinearAlgebra: ldiv!
 
 export block_gmres, block_bicgstab, ilu0, ic0, CUSOLVERRF, BatchPlan, batch_solve!, BlockJacobiPreconditioner
 export PowerFlowAssembly, mismatch!, jacobian!
+export WarmStartMLP, set_scale!, warm_start, train_step!, deflation_basis, judged_warm_start, learned_solve
 
 const libbpf = joinpath(@__DIR__, "..", "lib", "libbpf.so")
 
@@ -326,6 +327,75 @@ function jacobian!(PF::PowerFlowAssembly, x::CuVector{Float64}, Gu::Union{Nothin
                 PF.h, pointer(x), pointer(nonzeros(PF.Gx)), Gu === nothing ? CU_NULL : pointer(Gu),
                 Gu === nothing ? 0 : stride(Gu, 2)))
     return PF.Gx
+end
+
+# ---- learned warm start and deflation basis (an addition) ----------------------------------
+# A 3-layer MLP (n -> hidden -> hidden -> n, BF16 weights, tensor-core products, Adam) trained on
+# the solver's own (b, x) pairs; block-GMRES runs from its judged warm start with its deflation
+# basis, to the requested residual whatever the network predicts.
+mutable struct WarmStartMLP
+    h::Ptr{Cvoid}
+    n::Int
+end
+
+function WarmStartMLP(n::Int; hidden::Int=512, seed::Integer=0)
+    hidden % 128 == 0 || throw(ArgumentError("hidden must be a multiple of 128"))
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:bpf_mlp_create, libbpf), Cint, (Ptr{Cvoid}, Cint, Cint, Culonglong, Ref{Ptr{Cvoid}}),
+                ctx(), n, hidden, seed, r))
+    M = WarmStartMLP(r[], n)
+    finalizer(m -> ccall((:bpf_mlp_destroy, libbpf), Cint, (Ptr{Cvoid},), m.h), M)
+    return M
+end
+
+# the output scale: the training set's typical ||x|| / ||b||
+set_scale!(M::WarmStartMLP, s::Real) =
+    check(ccall((:bpf_mlp_set_scale, libbpf), Cint, (Ptr{Cvoid}, Cdouble), M.h, s))
+
+function warm_start(M::WarmStartMLP, B::CuMatrix{Float64})
+    size(B, 1) == M.n || throw(DimensionMismatch("B has $(size(B, 1)) rows, the network $(M.n)"))
+    X = CuMatrix{Float64}(undef, size(B)...)
+    check(ccall((:bpf_mlp_forward, libbpf), Cint,
+                (Ptr{Cvoid}, Cint, CuPtr{Cdouble}, Cint, CuPtr{Cdouble}, Cint),
+                M.h, size(B, 2), pointer(B), stride(B, 2), pointer(X), stride(X, 2)))
+    return X
+end
+
+# one Adam step on the pairs (B, X), at most 128 columns; returns the batch loss
+function train_step!(M::WarmStartMLP, B::CuMatrix{Float64}, X::CuMatrix{Float64}; lr::Float64=2e-4)
+    size(B) == size(X) || throw(DimensionMismatch("B and X differ in size"))
+    loss = Ref{Cdouble}(0.0)
+    check(ccall((:bpf_mlp_train_step, libbpf), Cint,
+                (Ptr{Cvoid}, Cint, CuPtr{Cdouble}, Cint, CuPtr{Cdouble}, Cint, Cdouble, Ref{Cdouble}),
+                M.h, size(B, 2), pointer(B), stride(B, 2), pointer(X), stride(X, 2), lr, loss))
+    return loss[]
+end
+
+# orthonormal n x rank basis of the network's outputs on Gaussian probes
+function deflation_basis(M::WarmStartMLP, rank::Int; seed::Integer=0)
+    Z = CuMatrix{Float64}(undef, M.n, rank)
+    check(ccall((:bpf_mlp_basis, libbpf), Cint, (Ptr{Cvoid}, Cint, Culonglong, CuPtr{Cdouble}, Cint),
+                M.h, rank, seed, pointer(Z), stride(Z, 2)))
+    return Z
+end
+
+# the network's warm start if its residual ||B - A X0|| is below ||B|| (the zero start's), else nothing
+function judged_warm_start(M::WarmStartMLP, A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64})
+    X0 = warm_start(M, B)
+    R = copy(B)
+    check(ccall((:bpf_spmm, libbpf), Cint,
+                (Ptr{Cvoid}, Ref{CsrDesc}, Cint, Cdouble, CuPtr{Cdouble}, Cint, Cdouble, CuPtr{Cdouble}, Cint),
+                ctx(), Ref(desc(A)), size(X0, 2), -1.0, pointer(X0), stride(X0, 2), 1.0, pointer(R), stride(R, 2)))
+    return norm(R) < norm(B) ? X0 : nothing
+end
+
+# right-preconditioned block-GMRES from the judged warm start, with the deflation basis Z if given;
+# tolerance rtol ||B||_F whatever the start
+function learned_solve(A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64}, N, M::WarmStartMLP;
+                       Z::Union{Nothing,CuMatrix{Float64}}=nothing, rtol::Float64=1e-8, itmax::Int=300)
+    X0 = judged_warm_start(M, A, B)
+    return block_gmres(A, B, X0; N=N, ldiv=true, restart=false, memory=itmax, atol=rtol * norm(B),
+                       rtol=0.0, itmax=itmax, deflation=Z)
 end
 
 # ---- block-BiCGSTAB (src/block_bicgstab.jl:182-299) -----------------------------------

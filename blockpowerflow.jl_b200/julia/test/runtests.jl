@@ -6,7 +6,7 @@
 #   julia --project=<env with CUDA.jl> blockpowerflow.jl_b200/julia/test/runtests.jl
 #
 # libbpf.so must be built first (make -C blockpowerflow.jl_b200/csrc).
-using Test, LinearAlgebra, SparseArrays, Random
+using Test, LinearAlgebra, SparseArrays, Random, Statistics
 using CUDA, CUDA.CUSPARSE
 
 include(joinpath(@__DIR__, "..", "BlockPowerFlowB200.jl"))
@@ -151,4 +151,20 @@ end
     Jd = SparseMatrixCSC(Gx)
     @test Matrix(Jd) ≈ J rtol = 1e-6
     @test all(isfinite, Array(Gu))
+end
+
+@testset "learned warm start and deflation basis" begin
+    M = WarmStartMLP(n; hidden=128, seed=1)
+    P = ilu0(Ad, 32)
+    X, st = block_gmres(Ad, Bd; N=P, ldiv=true, atol=0.0, rtol=1e-10, itmax=200, memory=200)
+    set_scale!(M, median(norm.(eachcol(Array(X)))))
+    losses = [train_step!(M, Bd, X; lr=1e-3) for _ in 1:20]
+    @test all(isfinite, losses)
+    X0 = warm_start(M, Bd)
+    @test size(X0) == size(Bd)
+    Z = deflation_basis(M, 8)
+    @test Array(Z)' * Array(Z) ≈ Matrix{Float64}(I, 8, 8) atol = 1e-10
+    Xl, stl = learned_solve(Ad, Bd, P, M; Z=Z, rtol=1e-8)
+    @test stl.solved
+    @test norm(B - A * Array(Xl)) <= 1e-7 * norm(B)   # stopping test on the estimate, 1e-8
 end

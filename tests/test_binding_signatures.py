@@ -72,7 +72,7 @@ def _julia_kind(t):
         return "ptr"
     if t in ("Cdouble", "Float64"):
         return "double"
-    if t in ("Clonglong", "Int64"):
+    if t in ("Clonglong", "Culonglong", "Int64", "UInt64"):
         return "int64"
     if t in ("Cint", "Int32"):
         return "int"
