@@ -15,6 +15,7 @@ using SparseArrays
 import LinearAlgebra: ldiv!
 
 export block_gmres, block_bicgstab, ilu0, ic0, CUSOLVERRF, BatchPlan, batch_solve!, BlockJacobiPreconditioner
+export householder, householder!
 export PowerFlowAssembly, mismatch!, jacobian!
 export WarmStartMLP, set_scale!, warm_start, train_step!, deflation_basis, judged_warm_start, learned_solve
 
@@ -397,6 +398,27 @@ function learned_solve(A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64},
     return block_gmres(A, B, X0; N=N, ldiv=true, restart=false, memory=itmax, atol=rtol * norm(B),
                        rtol=0.0, itmax=itmax, deflation=Z)
 end
+
+# ---- householder (src/block_utils.jl:38-53) ----------------------------------------------
+# Reduced QR of an n x k device block: Q overwritten by the orthonormal factor, R (k x k) upper
+# triangular with Q R = A.  Computed as Cholesky-QR2, so R's diagonal is positive (LAPACK's may be
+# negative: Q and R differ from geqrf/orgqr's by the same diagonal +-1 scaling) and no reflectors
+# are formed: tau is left as it is and compact = true is not available.
+function householder!(Q::CuMatrix{Float64}, R::CuMatrix{Float64},
+                      tau::CuVector{Float64}=CuVector{Float64}(undef, 0); compact::Bool=false)
+    compact && throw(ArgumentError("compact = true (the Householder reflectors) is not produced by this build"))
+    n, k = size(Q)
+    n >= k || throw(DimensionMismatch("householder needs n >= k"))
+    size(R) == (k, k) || throw(DimensionMismatch("R must be $k x $k"))
+    fill!(R, 0.0)
+    check(ccall((:bpf_householder, libbpf), Cint,
+                (Ptr{Cvoid}, Cint, Cint, CuPtr{Cdouble}, Cint, CuPtr{Cdouble}, Cint),
+                ctx(), n, k, pointer(Q), stride(Q, 2), pointer(R), stride(R, 2)))
+    return Q, R
+end
+
+householder(A::CuMatrix{Float64}; compact::Bool=false) =
+    householder!(copy(A), CuMatrix{Float64}(undef, size(A, 2), size(A, 2)); compact)
 
 # ---- block-BiCGSTAB (src/block_bicgstab.jl:182-299) -----------------------------------
 function block_bicgstab(A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64};

@@ -49,6 +49,17 @@ const Bd = CuMatrix(B)
     @test_throws ErrorException block_gmres(Ad, CuMatrix(zeros(n + 1, 2)))
 end
 
+@testset "householder (src/block_utils.jl:38-53)" begin
+    W = randn(MersenneTwister(4), n, 16)
+    Q, R = householder(CuMatrix(W))
+    Qh, Rh = Array(Q), Array(R)
+    @test Qh' * Qh ≈ Matrix{Float64}(I, 16, 16) atol = 1e-12
+    @test Qh * Rh ≈ W
+    @test istriu(Rh)
+    @test all(diag(Rh) .> 0)
+    @test_throws ArgumentError householder(CuMatrix(W); compact=true)
+end
+
 @testset "block_bicgstab (test/block_bicgstab.jl settings)" begin
     P = ilu0(Ad, 32)
     X, st = block_bicgstab(Ad, Bd; N=P, atol=1e-8, rtol=0.0, itmax=500)
