@@ -10,7 +10,8 @@ from . import grid
 from .batch import BatchPlan, BatchStats, autotune
 from ._lib import (BPFError, DimensionMismatch, SingularException, exported_symbols,
                    kernel_launches)
-from .krylov import BlockGMRESStats, SimpleStats, block_bicgstab, block_gmres
+from .krylov import (BlockBicgstabSolver, BlockGMRESSolver, BlockGMRESStats, SimpleStats, block_bicgstab,
+                     block_bicgstab_, block_gmres, block_gmres_, warm_start_)
 from .precond import NVIDIA_IC0, NVIDIA_ILU0, BlockJacobiPreconditioner, ic0, ilu0, ldiv_, mul_
 from .sparse import CuSparseMatrixCSR, colmajor, empty_colmajor, householder, mul
 
@@ -21,5 +22,6 @@ __all__ = [
     "ldiv", "NVIDIA_ILU0", "NVIDIA_IC0", "CuSparseMatrixCSR", "mul", "householder", "colmajor",
     "empty_colmajor", "BPFError", "DimensionMismatch", "SingularException", "grid",
     "exported_symbols", "kernel_launches", "CUSOLVERRF", "BatchPlan", "BatchStats", "autotune",
-    "BlockJacobiPreconditioner", "mul_",
+    "BlockJacobiPreconditioner", "mul_", "BlockGMRESSolver", "BlockBicgstabSolver", "block_gmres_",
+    "block_bicgstab_", "warm_start_",
 ]

@@ -135,3 +135,107 @@ def block_bicgstab(A: CuSparseMatrixCSR, B, *, C=None, N=None, atol: float = _SQ
                         res[: min(st.n_residuals, len(res))].tolist() if history else [],
                         st.timer, _status_string(st.status))
     return X, stats
+
+
+# ---- in-place forms: solver objects, block_gmres! / block_bicgstab!, warm_start! ----------------
+
+
+def _device_of(B):
+    """The solution block follows B (the reference allocates it with B's type); host arrays -> cuda."""
+    import torch
+
+    return B.device if isinstance(B, torch.Tensor) else torch.device("cuda")
+
+
+class BlockGMRESSolver:
+    """BlockGMRESSolver (src/block_gmres.jl:21-68): the block a solve writes its solution into
+    (X, n x p, column-major), the statistics of the last solve, the basis size `memory` (clamped
+    to div(n, p) as the reference does) and a pending warm start.  The Krylov basis and the small
+    blocks live in the library's per-device context and are reused from solve to solve, so they
+    are not fields here.  BlockGMRESSolver(A, B; memory=5), or from_sizes(m, n, p, memory)."""
+
+    def __init__(self, A, B, *, memory: int = 5):
+        m, n = A.shape
+        s, p = B.shape
+        self._init(m, n, p, memory, _device_of(B))
+
+    @classmethod
+    def from_sizes(cls, m: int, n: int, p: int, memory: int, device=None):
+        """BlockGMRESSolver(m, n, p, memory, SV, SM)."""
+        import torch
+
+        self = cls.__new__(cls)
+        self._init(m, n, p, memory, torch.device("cuda") if device is None else torch.device(device))
+        return self
+
+    def _init(self, m, n, p, memory, device):
+        self.m, self.n, self.p = int(m), int(n), int(p)
+        self.memory = min(n // max(p, 1), int(memory))
+        self.device = device
+        self.X = empty_colmajor(self.n, self.p, device)
+        self.dX = None
+        self.warm_start = False
+        self.stats = BlockGMRESStats(0, False, [], 0.0, "unknown")
+
+
+def warm_start_(solver: BlockGMRESSolver, X0) -> BlockGMRESSolver:
+    """warm_start!(solver, X0) (src/block_gmres.jl:70-79): the next block_gmres_ starts from X0."""
+    n, p = solver.n, solver.p
+    if tuple(X0.shape) != (n, p):
+        raise _lib.DimensionMismatch(_lib.BPF_ERR_DIMENSION, f"X0 should have size ({n}, {p})")
+    solver.dX = colmajor(X0, device=solver.device).clone()
+    solver.warm_start = True
+    return solver
+
+
+def block_gmres_(solver: BlockGMRESSolver, A: CuSparseMatrixCSR, B, X0=None, *, M=None, N=None,
+                 ldiv: bool = False, restart: bool = False, reorthogonalization: bool = False,
+                 atol: float = _SQRT_EPS, rtol: float = _SQRT_EPS, itmax: int = 0,
+                 timemax: float = math.inf, verbose: int = 0, history: bool = False) -> BlockGMRESSolver:
+    """block_gmres!(solver, A, B[, X0]; kwargs...) (src/block_gmres.jl:97-411): the solve with
+    the solver's basis size; the solution goes into solver.X, the statistics into solver.stats,
+    and a warm start (X0 here or an earlier warm_start_) is consumed.  Returns the solver."""
+    if X0 is not None:
+        warm_start_(solver, X0)
+    s, p = B.shape
+    if (s, p) != (solver.n, solver.p):
+        raise _lib.DimensionMismatch(_lib.BPF_ERR_DIMENSION,
+                                     f"B is {s} x {p}, the solver was built for {solver.n} x {solver.p}")
+    X, st = block_gmres(A, B, solver.dX if solver.warm_start else None, memory=solver.memory, M=M, N=N,
+                        ldiv=ldiv, restart=restart, reorthogonalization=reorthogonalization, atol=atol,
+                        rtol=rtol, itmax=itmax, timemax=timemax, verbose=verbose, history=history)
+    solver.X.copy_(X)
+    solver.stats = st
+    solver.warm_start = False
+    solver.dX = None
+    return solver
+
+
+class BlockBicgstabSolver:
+    """BlockBicgstabSolver (src/block_bicgstab.jl:23-55): the solution block X (n x p,
+    column-major) and the statistics of the last solve; the iteration's blocks live in the
+    library's per-device context."""
+
+    def __init__(self, A, B):
+        n, m = A.shape
+        s, p = B.shape
+        self.n, self.p = int(n), int(p)
+        self.device = _device_of(B)
+        self.X = empty_colmajor(self.n, self.p, self.device)
+        self.stats = SimpleStats(0, False, [], 0.0, "unknown")
+
+
+def block_bicgstab_(solver: BlockBicgstabSolver, A: CuSparseMatrixCSR, B, *, C=None, N=None,
+                    atol: float = _SQRT_EPS, rtol: float = _SQRT_EPS, itmax: int = 0,
+                    timemax: float = math.inf, verbose: int = 0, history: bool = False):
+    """block_bicgstab!(solver, A, B; C=B, N, kwargs...) (src/block_bicgstab.jl:187-299): the
+    solution into solver.X, the statistics into solver.stats; returns (X, stats) as there."""
+    s, p = B.shape
+    if (s, p) != (solver.n, solver.p):
+        raise _lib.DimensionMismatch(_lib.BPF_ERR_DIMENSION,
+                                     f"B is {s} x {p}, the solver was built for {solver.n} x {solver.p}")
+    X, st = block_bicgstab(A, B, C=C, N=N, atol=atol, rtol=rtol, itmax=itmax, timemax=timemax,
+                           verbose=verbose, history=history)
+    solver.X.copy_(X)
+    solver.stats = st
+    return solver.X, solver.stats

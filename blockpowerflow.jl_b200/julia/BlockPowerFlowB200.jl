@@ -16,6 +16,7 @@ import LinearAlgebra: ldiv!
 
 export block_gmres, block_bicgstab, ilu0, ic0, CUSOLVERRF, BatchPlan, batch_solve!, BlockJacobiPreconditioner
 export householder, householder!
+export BlockGMRESSolver, block_gmres!, warm_start!, BlockBicgstabSolver, block_bicgstab!
 export PowerFlowAssembly, mismatch!, jacobian!
 export WarmStartMLP, set_scale!, warm_start, train_step!, deflation_basis, judged_warm_start, learned_solve
 
@@ -228,6 +229,70 @@ function block_gmres(A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64},
                                      history ? res[1:min(s.n_residuals, cap)] : Float64[],
                                      s.timer, status_string(s.status))
     return X, stats
+end
+
+# ---- in-place forms (src/block_gmres.jl:21-168,397-411; src/block_bicgstab.jl:23-55,187-299) -----
+# The solver objects hold the solution block, the statistics and (GMRES) the basis size and a
+# pending warm start; the Krylov basis and the small blocks live in the library's context.
+mutable struct BlockGMRESSolver
+    m::Int
+    n::Int
+    p::Int
+    memory::Int
+    X::CuMatrix{Float64}
+    ΔX::Union{Nothing,CuMatrix{Float64}}
+    warm_start::Bool
+    stats::BlockGMRESStats{Float64}
+end
+
+BlockGMRESSolver(m::Int, n::Int, p::Int, memory::Int) =
+    BlockGMRESSolver(m, n, p, min(div(n, p), memory), CuMatrix{Float64}(undef, n, p), nothing, false,
+                     BlockGMRESStats{Float64}(0, false, Float64[], 0.0, "unknown"))
+BlockGMRESSolver(A, B; memory::Int=5) = BlockGMRESSolver(size(A, 1), size(A, 2), size(B, 2), memory)
+
+function warm_start!(solver::BlockGMRESSolver, X0::CuMatrix{Float64})
+    n, p = size(solver.X)
+    size(X0) == (n, p) || error("X0 should have size ($n, $p)")
+    solver.ΔX = copy(X0)
+    solver.warm_start = true
+    return solver
+end
+
+function block_gmres!(solver::BlockGMRESSolver, A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64},
+                      X0::CuMatrix{Float64}; kwargs...)
+    warm_start!(solver, X0)
+    return block_gmres!(solver, A, B; kwargs...)
+end
+
+function block_gmres!(solver::BlockGMRESSolver, A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64};
+                      M=I, N=I, ldiv::Bool=false, restart::Bool=false, reorthogonalization::Bool=false,
+                      atol::Float64=√eps(Float64), rtol::Float64=√eps(Float64), itmax::Int=0,
+                      timemax::Float64=Inf, verbose::Int=0, history::Bool=false)
+    size(B) == size(solver.X) || error("Inconsistent problem size")
+    X, stats = block_gmres(A, B, solver.warm_start ? solver.ΔX : nothing; memory=solver.memory, M, N, ldiv,
+                           restart, reorthogonalization, atol, rtol, itmax, timemax, verbose, history)
+    copyto!(solver.X, X)
+    solver.stats = stats
+    solver.warm_start = false
+    solver.ΔX = nothing
+    return solver
+end
+
+mutable struct BlockBicgstabSolver
+    X::CuMatrix{Float64}
+    stats::SimpleStats{Float64}
+end
+
+BlockBicgstabSolver(A, B) = BlockBicgstabSolver(CuMatrix{Float64}(undef, size(A, 1), size(B, 2)),
+                                                SimpleStats{Float64}(0, false, Float64[], 0.0, "unknown"))
+
+function block_bicgstab!(solver::BlockBicgstabSolver, A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64};
+                         kwargs...)
+    size(B) == size(solver.X) || error("Inconsistent problem size")
+    X, stats = block_bicgstab(A, B; kwargs...)
+    copyto!(solver.X, X)
+    solver.stats = stats
+    return (solver.X, solver.stats)
 end
 
 # ---- batched block-GMRES (an addition: many systems in one graph launch) ----------------

@@ -49,6 +49,22 @@ const Bd = CuMatrix(B)
     @test_throws ErrorException block_gmres(Ad, CuMatrix(zeros(n + 1, 2)))
 end
 
+@testset "in-place forms: BlockGMRESSolver, block_gmres!, warm_start!, block_bicgstab!" begin
+    P = ilu0(Ad, 32)
+    solver = BlockGMRESSolver(Ad, Bd; memory=50)
+    @test solver.memory == div(n, 32)
+    block_gmres!(solver, Ad, Bd; N=P, ldiv=true, atol=1e-8, rtol=0.0, itmax=500)
+    @test solver.stats.solved
+    X1 = Array(solver.X)
+    @test norm(B - A * X1) <= 1e-7
+    block_gmres!(solver, Ad, Bd, CuMatrix(X1); N=P, ldiv=true, atol=1e-8, rtol=0.0, itmax=500)
+    @test solver.stats.solved && solver.stats.niter <= 1 && !solver.warm_start
+    @test_throws ErrorException warm_start!(solver, CuMatrix(zeros(n, 3)))
+    bsolver = BlockBicgstabSolver(Ad, Bd)
+    X, st = block_bicgstab!(bsolver, Ad, Bd; N=P, atol=1e-8, rtol=0.0, itmax=500)
+    @test X === bsolver.X && st.solved
+end
+
 @testset "householder (src/block_utils.jl:38-53)" begin
     W = randn(MersenneTwister(4), n, 16)
     Q, R = householder(CuMatrix(W))
