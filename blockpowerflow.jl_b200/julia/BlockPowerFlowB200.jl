@@ -147,6 +147,13 @@ function ic0(A::CuSparseMatrixCSR{Float64,Cint}, nrhs::Int; factor_type=Float64,
     return P
 end
 
+# CSC input, which the reference's ilu0 / ic0 accept (src/preconditioners_nvidia.jl:6,42): there
+# the factors are those of A^T and are applied transposed.  The incomplete factorization whose
+# product matches A on A's pattern is unique, so that is the same preconditioner as the CSR
+# form's; the matrix is converted to CSR once (the library keeps no pointer to it).
+ilu0(A::CuSparseMatrixCSC{Float64,Cint}, nrhs::Int; kwargs...) = ilu0(CuSparseMatrixCSR(A), nrhs; kwargs...)
+ic0(A::CuSparseMatrixCSC{Float64,Cint}, nrhs::Int; kwargs...) = ic0(CuSparseMatrixCSR(A), nrhs; kwargs...)
+
 function ldiv!(y::CuVecOrMat{Float64}, P::DevicePrec, x::CuVecOrMat{Float64})
     p = size(x, 2)
     check(ccall((:bpf_prec_apply, libbpf), Cint,

@@ -91,6 +91,10 @@ end
         ldiv!(y, P, x)
         @test all(isfinite, Array(y))
     end
+    Pr, Pc = ilu0(Ad, 4), ilu0(CuSparseMatrixCSC(A), 4)   # CSR and CSC input: the same ILU(0)
+    yr, yc = similar(x), similar(x)
+    ldiv!(yr, Pr, x); ldiv!(yc, Pc, x)
+    @test Array(yc) ≈ Array(yr)
     S = A + A' + 2I                             # symmetric positive definite
     Sd = CuSparseMatrixCSR(S)
     C = ic0(Sd, 32)
