@@ -23,3 +23,18 @@ def test_batch_workload_matches_the_configuration():
     b2, p2, m2, B2 = bench.batch_workload(16, seed=0)
     assert list(b2) == list(buses) and p2 == nrhs
     assert all((x != y).nnz == 0 for x, y in zip(mats, m2)) and all(np.array_equal(x, y) for x, y in zip(Bs, B2))
+
+
+def test_cpu_baseline_times_the_whole_solve_when_it_is_short():
+    """The oracle's solve of a small system is predicted well under the bound, so the baseline
+    runs it to the tolerance and reports its real iteration count; the extrapolation is the
+    fallback for long solves."""
+    import bench
+    from blockpowerflow_b200 import grid as g
+
+    J = g.preset_jacobian("case300", 0)
+    B = g.gaussian_rhs(J.shape[0], 8, 3)
+    cb = bench.cpu_baseline(J, B, 25, 2)
+    assert cb["kind"] == "port" and cb["cores"] == 2 and cb["value"] > 0
+    assert "the whole solve" in cb["sample"] and cb["iterations"] > 0
+    assert abs(cb["value"] - B.shape[1] / cb["seconds_per_solve"]) <= 1e-9 * cb["value"]
