@@ -22,6 +22,7 @@
 #include <climits>
 #include <cmath>
 #include <numeric>
+#include <system_error>
 #include <thread>
 
 #include "bpf_internal.cuh"
@@ -180,23 +181,23 @@ bool build_pairs(int n, const int *rp, const int *ci, const int *diag, bool ic,
     const unsigned hw = std::thread::hardware_concurrency();
     const int nthreads = nnz >= 200000 ? (int)std::min(16u, std::max(1u, hw)) : 1;
     auto run = [&](int pass) {
-        if (nthreads <= 1) {
-            std::vector<int> pos(n, -1);
-            rows(pass, 0, n, pos);
-            return;
-        }
         std::atomic<int> next(0);
+        auto work = [&]() {
+            std::vector<int> pos(n, -1);
+            for (;;) {
+                const int b = next.fetch_add(64);
+                if (b >= n) break;
+                rows(pass, b, std::min(n, b + 64), pos);
+            }
+        };
         std::vector<std::thread> pool;
-        pool.reserve(nthreads);
-        for (int t = 0; t < nthreads; t++)
-            pool.emplace_back([&]() {
-                std::vector<int> pos(n, -1);
-                for (;;) {
-                    const int b = next.fetch_add(64);
-                    if (b >= n) break;
-                    rows(pass, b, std::min(n, b + 64), pos);
-                }
-            });
+        try {
+            for (int t = 1; t < nthreads; t++) pool.emplace_back(work);
+        } catch (const std::system_error &) {
+            // fewer helpers than asked (a thread limit): the calling thread still takes every
+            // block the helpers do not
+        }
+        work();
         for (auto &th : pool) th.join();
     };
     run(0);
