@@ -38,3 +38,23 @@ def test_cpu_baseline_times_the_whole_solve_when_it_is_short():
     assert cb["kind"] == "port" and cb["cores"] == 2 and cb["value"] > 0
     assert "the whole solve" in cb["sample"] and cb["iterations"] > 0
     assert abs(cb["value"] - B.shape[1] / cb["seconds_per_solve"]) <= 1e-9 * cb["value"]
+
+
+def test_reference_arm_prints_one_contract_line():
+    """bench.py --impl reference: the oracle on the host cores, one JSON line with the keys the
+    benchmark contract names (no GPU needed)."""
+    import json
+    import subprocess
+
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=600,
+                         cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+              "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
