@@ -101,13 +101,27 @@ def control_jacobian(prob: PowerFlowProblem, x: np.ndarray) -> np.ndarray:
     dS/d|V| = diag(V) conj(Ybus diag(V / |V|)) + conj(diag(Ybus V)) diag(V / |V|)."""
     g = prob.grid
     vm, va = state_to_voltages(prob, x)
-    Y = g.ybus()
+    Y = g.ybus().tocsc()
     V = vm * np.exp(1j * va)
     I = Y @ V
     Vn = V / np.abs(V)
-    dS = (sp.diags(V) @ (Y @ sp.diags(Vn)).conj() + sp.diags(I.conj()) @ sp.diags(Vn)).tocsc()
-    cols = dS[:, prob.ctrl].toarray()
-    return np.vstack([cols.real[1:], cols.imag[g.pq]])
+    # only the control columns: the entries of Y(:, ctrl), then the diagonal terms
+    sub = Y[:, prob.ctrl]
+    rows = sub.indices
+    j = np.repeat(np.arange(len(prob.ctrl)), np.diff(sub.indptr))
+    k = prob.ctrl[j]
+    vals = V[rows] * np.conj(sub.data * Vn[k])
+    nb, nc = g.n_bus, len(prob.ctrl)
+    # written straight into [P rows (buses 1..nb-1); Q rows (PQ buses)]
+    qrow = np.full(nb, -1)
+    qrow[g.pq] = nb - 1 + np.arange(len(g.pq))
+    out = np.zeros((nb - 1 + len(g.pq), nc))
+    for r, c, v in ((rows, j, vals), (prob.ctrl, np.arange(nc), np.conj(I[prob.ctrl]) * Vn[prob.ctrl])):
+        p_ok = r >= 1
+        np.add.at(out, (r[p_ok] - 1, c[p_ok]), v.real[p_ok])
+        q_ok = qrow[r] >= 0
+        np.add.at(out, (qrow[r[q_ok]], c[q_ok]), v.imag[q_ok])
+    return out
 
 
 def bus_arrays(prob: PowerFlowProblem):
