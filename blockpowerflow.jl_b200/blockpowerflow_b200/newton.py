@@ -90,10 +90,69 @@ def mismatch(prob: PowerFlowProblem, x: np.ndarray) -> np.ndarray:
     return np.concatenate([d.real[1:], d.imag[prob.grid.pq]])
 
 
+def _coupling(prob: PowerFlowProblem):
+    """Ybus (CSR, duplicates summed) and, per Ybus entry (i, k), the positions in prob.pattern of
+    (P_i | Q_i) x (theta_k | |V|_k) (-1 where the row or column is not an unknown); built once per
+    pattern and kept on the problem.  None if a nonempty Ybus row lacks its diagonal (the I_i terms
+    attach there)."""
+    key = (id(prob.pattern), prob.pattern.nnz)
+    cached = prob.__dict__.get("_coupling_cache")
+    if cached is not None and cached[0] == key:
+        return cached[1]
+    g = prob.grid
+    nb = g.n_bus
+    Y = g.ybus().tocsr()
+    Y.sum_duplicates()
+    Y.sort_indices()
+    rows = np.repeat(np.arange(nb), np.diff(Y.indptr))
+    cols = Y.indices
+    has_diag = np.zeros(nb, dtype=bool)
+    has_diag[rows[rows == cols]] = True
+    if np.any(~has_diag & (np.diff(Y.indptr) > 0)):
+        prob.__dict__["_coupling_cache"] = (key, None)
+        return None
+    prow = np.arange(nb) - 1                      # P row / theta column of bus i (-1: slack)
+    qrow = np.full(nb, -1)
+    qrow[g.pq] = nb - 1 + np.arange(len(g.pq))    # Q row / |V| column of a PQ bus
+    P = prob.pattern
+    n = P.shape[0]
+    keys = np.repeat(np.arange(n, dtype=np.int64), np.diff(P.indptr)) * n + P.indices
+    maps = []
+    for r, c in ((prow[rows], prow[cols]), (prow[rows], qrow[cols]), (qrow[rows], prow[cols]), (qrow[rows], qrow[cols])):
+        ok = (r >= 0) & (c >= 0)
+        k = r.astype(np.int64) * n + c
+        pos = np.searchsorted(keys, k)
+        pos = np.minimum(pos, len(keys) - 1)
+        found = ok & (keys[pos] == k)
+        if np.any(ok & ~found & (Y.data != 0)):
+            raise ValueError("the Jacobian left the fixed sparsity pattern")
+        maps.append(np.where(found, pos, -1))
+    out = (Y, rows, cols, maps)
+    prob.__dict__["_coupling_cache"] = (key, out)
+    return out
+
+
 def jacobian_values(prob: PowerFlowProblem, x: np.ndarray) -> np.ndarray:
-    """Gx's values on the fixed pattern (CSR order)."""
+    """Gx's values on the fixed pattern (CSR order): per Ybus entry (i, k),
+    dS_i/dtheta_k = j V_i ([i == k] conj(I_i) - conj(Y_ik V_k)) and
+    dS_i/d|V_k| = V_i conj(Y_ik V_k / |V_k|) + [i == k] conj(I_i) V_i / |V_i|, scattered through
+    the position map of _coupling (the assembly the device runs)."""
     vm, va = state_to_voltages(prob, x)
-    return G.jacobian_on_pattern(prob.grid, prob.pattern, vm, va)
+    cpl = _coupling(prob)
+    if cpl is None:
+        return G.jacobian_on_pattern(prob.grid, prob.pattern, vm, va)
+    Y, rows, cols, maps = cpl
+    V = vm * np.exp(1j * va)
+    I = Y @ V
+    y = Y.data
+    diag = rows == cols
+    dth = 1j * V[rows] * (np.where(diag, np.conj(I[rows]), 0) - np.conj(y * V[cols]))
+    dm = V[rows] * np.conj(y * V[cols] / np.abs(V[cols])) + np.where(diag, np.conj(I[rows]) * V[rows] / np.abs(V[rows]), 0)
+    out = np.zeros(prob.pattern.nnz)
+    for m, v in zip(maps, (dth.real, dm.real, dth.imag, dm.imag)):
+        ok = m >= 0
+        out[m[ok]] = v[ok]
+    return out
 
 
 def control_jacobian(prob: PowerFlowProblem, x: np.ndarray) -> np.ndarray:
