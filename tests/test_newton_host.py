@@ -74,3 +74,16 @@ def test_newton_converges_quadratically_with_a_stand_in_solver(prob):
     r2 = NT.newton(p2, solver=_SciPyStandIn(prob.pattern), tol=1e-12, x0=r.x)
     fd = (r2.x - r.x) / h
     assert np.linalg.norm(r.sensitivities[:, 1] - fd) <= 1e-4 * np.linalg.norm(fd)
+
+
+def test_jacobian_values_match_the_sparse_product_jacobian(prob):
+    """The position-map assembly of jacobian_values equals grid.jacobian_on_pattern (the sparse
+    matrix-product form) on the fixed pattern, and its map is built once per problem."""
+    x = NT.perturbed_start(prob, 0.05, seed=4)
+    vm, va = NT.state_to_voltages(prob, x)
+    ref = G.jacobian_on_pattern(prob.grid, prob.pattern, vm, va)
+    got = NT.jacobian_values(prob, x)
+    assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
+    cached = prob.__dict__["_coupling_cache"]
+    NT.jacobian_values(prob, NT.perturbed_start(prob, 0.05, seed=5))
+    assert prob.__dict__["_coupling_cache"] is cached
