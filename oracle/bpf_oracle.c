@@ -231,9 +231,92 @@ void orc_prec_apply(int kind, int n, const int *rp, const int *ci, const double 
 /* ------------------------------------------------------------------------------------- */
 #define AT(A, ld, i, j) (A)[(size_t)(j) * (ld) + (i)]
 
+/* Cache-blocked products, switched on only to time the oracle as the CPU baseline (the checker
+ * keeps the plain loops below, so its rounding does not change): the same sums in another order. */
+static int g_fast_dense = 0;
+void orc_set_fast_dense(int on) { g_fast_dense = on != 0; }
+
+/* C = alpha A^T B + beta C, A k x m, B k x ncol: the k range split over the threads, each summing
+ * a private m x ncol block in 4 x 4 register tiles (16 independent sums per row of A and B). */
+static void gemm_tn_blocked(int m, int ncol, int k, double alpha, const double *A, int lda,
+                            const double *B, int ldb, double beta, double *C, int ldc) {
+    const int T = g_threads;
+    double *part = (double *)calloc((size_t)T * m * ncol, sizeof(double));
+#pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        const int l0 = (int)((long long)k * t / nt), l1 = (int)((long long)k * (t + 1) / nt);
+        double *P = part + (size_t)t * m * ncol;
+        for (int j0 = 0; j0 < ncol; j0 += 4) {
+            const int jb = ncol - j0 < 4 ? ncol - j0 : 4;
+            for (int i0 = 0; i0 < m; i0 += 4) {
+                const int ib = m - i0 < 4 ? m - i0 : 4;
+                double acc[4][4] = {{0}};
+                if (ib == 4 && jb == 4) {
+                    const double *a0 = A + (size_t)i0 * lda, *a1 = a0 + lda, *a2 = a1 + lda, *a3 = a2 + lda;
+                    const double *b0 = B + (size_t)j0 * ldb, *b1 = b0 + ldb, *b2 = b1 + ldb, *b3 = b2 + ldb;
+                    for (int l = l0; l < l1; l++) {
+                        const double x0 = a0[l], x1 = a1[l], x2 = a2[l], x3 = a3[l];
+                        const double y0 = b0[l], y1 = b1[l], y2 = b2[l], y3 = b3[l];
+                        acc[0][0] += x0 * y0; acc[0][1] += x0 * y1; acc[0][2] += x0 * y2; acc[0][3] += x0 * y3;
+                        acc[1][0] += x1 * y0; acc[1][1] += x1 * y1; acc[1][2] += x1 * y2; acc[1][3] += x1 * y3;
+                        acc[2][0] += x2 * y0; acc[2][1] += x2 * y1; acc[2][2] += x2 * y2; acc[2][3] += x2 * y3;
+                        acc[3][0] += x3 * y0; acc[3][1] += x3 * y1; acc[3][2] += x3 * y2; acc[3][3] += x3 * y3;
+                    }
+                } else {
+                    for (int ii = 0; ii < ib; ii++)
+                        for (int jj = 0; jj < jb; jj++) {
+                            const double *a = A + (size_t)(i0 + ii) * lda, *b = B + (size_t)(j0 + jj) * ldb;
+                            double s2 = 0.0;
+                            for (int l = l0; l < l1; l++) s2 += a[l] * b[l];
+                            acc[ii][jj] = s2;
+                        }
+                }
+                for (int ii = 0; ii < ib; ii++)
+                    for (int jj = 0; jj < jb; jj++) P[(size_t)(j0 + jj) * m + i0 + ii] = acc[ii][jj];
+            }
+        }
+    }
+    for (int j = 0; j < ncol; j++)
+        for (int i = 0; i < m; i++) {
+            double s2 = 0.0;
+            for (int t = 0; t < T; t++) s2 += part[(size_t)t * m * ncol + (size_t)j * m + i];
+            AT(C, ldc, i, j) = alpha * s2 + (beta == 0.0 ? 0.0 : beta * AT(C, ldc, i, j));
+        }
+    free(part);
+}
+
+/* C = alpha A B + beta C, A m x k, B k x ncol: blocks of 256 rows over the threads, each column
+ * of C updated by contiguous column streams of A (axpy form). */
+static void gemm_nn_blocked(int m, int ncol, int k, double alpha, const double *A, int lda,
+                            const double *B, int ldb, double beta, double *C, int ldc) {
+    const int nblk = (m + 255) / 256;
+#pragma omp parallel for num_threads(g_threads) schedule(static)
+    for (int b = 0; b < nblk; b++) {
+        const int i0 = b * 256, i1 = i0 + 256 < m ? i0 + 256 : m;
+        for (int j = 0; j < ncol; j++) {
+            double *c = C + (size_t)j * ldc;
+            if (beta == 0.0)
+                for (int i = i0; i < i1; i++) c[i] = 0.0;
+            else if (beta != 1.0)
+                for (int i = i0; i < i1; i++) c[i] *= beta;
+            for (int l = 0; l < k; l++) {
+                const double w = alpha * AT(B, ldb, l, j);
+                const double *a = A + (size_t)l * lda;
+                for (int i = i0; i < i1; i++) c[i] += w * a[i];
+            }
+        }
+    }
+}
+
 /* C = alpha * op(A) * B + beta * C ; op = A or A^T.  A is (ta? k x m : m x k). */
 static void gemm(int ta, int m, int ncol, int k, double alpha, const double *A, int lda,
                  const double *B, int ldb, double beta, double *C, int ldc) {
+    if (g_fast_dense && (size_t)m * ncol * k > 200000) {
+        if (ta) gemm_tn_blocked(m, ncol, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        else gemm_nn_blocked(m, ncol, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        return;
+    }
 #pragma omp parallel for num_threads(g_threads) schedule(static) if ((size_t)m * ncol * k > 200000)
     for (int j = 0; j < ncol; j++) {
         for (int i = 0; i < m; i++) {

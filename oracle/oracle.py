@@ -56,6 +56,12 @@ def set_threads(t: int) -> None:
     lib().orc_set_threads(int(t))
 
 
+def set_fast_dense(on: bool) -> None:
+    """Cache-blocked dense products (the same sums in another order), for timing the oracle as
+    the CPU baseline; the checker's default is the plain loops."""
+    lib().orc_set_fast_dense(int(bool(on)))
+
+
 def _ptr(a, ctype=C.c_double):
     return a.ctypes.data_as(C.POINTER(ctype))
 
