@@ -1,28 +1,34 @@
 #!/usr/bin/env python
-"""RHS solves/s at a 1e-8 relative residual on one B200 (one JSON line on stdout).
+"""RHS solves/s at a 1e-8 relative residual on B200 (one JSON line on stdout).
 
-Workload (the 9,000-bus grid of the second benchmark configuration): a seeded synthetic
-Newton power-flow Jacobian with 9,000 buses (16,998 unknowns, ~121k nonzeros) and 64 Gaussian
-right-hand sides, solved by block-GMRES with a right ILU(0) preconditioner, no restart (as in
-benchmarks_nvidia.jl), atol 0, rtol 1e-8.  One step = ILU(0) numeric refactorization of the
-Jacobian's values + the block-GMRES solve; the sparsity analysis is done once at set-up, as a
-Newton loop would.  RHS solves/s = converged right-hand sides / time.
+Default workload (the batched benchmark configuration): 512 independent synthetic power-flow
+grids of 100 - 3,000 buses (log-uniform, seeded; 909,646 unknowns in all) with 8 - 64 Gaussian
+right-hand sides each (18,919 in all), every system solved by ILU(0)-preconditioned block-GMRES
+(right preconditioner, ldiv, unrestarted) to ||B - A X||_F <= 1e-8 ||B||_F.  One step = the ILU(0)
+numeric factorization of every system + the solve of every right-hand side; the pattern analysis
+is set-up (a Newton loop pays it once per pattern).
 
-  value : device-resident inputs, CUDA-event time of K steps (max over ranks), L2 flushed
-          between steps (256 MB write).
-  e2e   : the same step through the public Python API with pinned host buffers: Jacobian
-          values and B copied host->device and X device->host inside the timed region.
-  roofline : the kernel class with the largest share of device time, measured live with
-          CUDA events around each of its launches inside the timed region.
-  cpu_baseline : the C restatement of the reference's block-GMRES (oracle/) on the host's
-          cores, first iterations of the same solve, scaled to the whole solve by operation
-          count.
+  value : the batched path (FP32 ILU(0) factors in minimum-degree order, FP64 residual and
+          orthogonalization, launch shape from the autotuner): one CUDA-graph launch per step,
+          device-resident blocks, CUDA events around each step (max over ranks), per-kernel
+          instrumentation off, L2 flushed between steps.
+  plain_fp64_dropin : the reference's call per system, block_gmres(A, B; N=ilu0(A, p), ldiv=true)
+          (FP64 natural-order ILU(0)), through this library on the same inputs in the same run.
+  e2e   : the batched path through the public API with pinned host blocks: every B copied
+          host -> device and every X device -> host inside the timed region.
+  err_vs_direct : ||X - X_direct||_F / ||X_direct||_F per system against SciPy's sparse LU
+          (FP64), computed outside the timed regions.
+  roofline : the persistent solve kernel, from a separate pass with per-kernel CUDA events.
+  cpu_baseline : the C restatement of the reference's block-GMRES + ILU(0) (oracle/) on the
+          host's cores, one system per thread, on every 8th system of the batch.
 
 `--impl reference` times that CPU restatement alone (the reference is Julia, and neither Julia
-nor its CUDA.jl stack is installed) on the same workload and prints the same metric with
-"impl":"reference".
-Multi-GPU (torchrun): every rank solves its own grid (seed offset by rank), no collective on
-the data path; value = all ranks' converged RHS / max-over-ranks time ("scaling": "weak").
+nor its CUDA.jl stack is installed) on the same 512 systems, every step a different 1/8 of them.
+Multi-GPU (torchrun): the 512 systems are shared out over the ranks by longest-processing-time
+assignment, no collective on the data path; value = all systems' converged RHS / max-over-ranks
+time ("scaling": "strong": the total work is fixed).
+
+`--config` names the other benchmark configurations (one line each, one GPU).
 """
 import argparse
 import json
@@ -44,11 +50,9 @@ RTOL = 1e-8
 ITMAX = 300
 CPU_SAMPLE_ITERS = (4, 10)
 CPU_FULL_MAX_S = 15.0   # the whole CPU solve is timed when predicted to take at most this long
-# DRAM bytes (read + write) per working launch of the FP64 product classes in the benchmark's
-# solve (minimum-degree ILU(0), 57 iterations), from one ncu capture of every launch
-# (profiles/launches_grid9k_p64_amd_ilu0_gmres.md): the kernels' total DRAM bytes over the
-# launches that always do their work, the ones bench.py's per-class timing counts.
-TRAFFIC_PER_LAUNCH = {"gram": 135.58e6, "tsmm": 126.28e6}
+NSYS = 512              # systems of the batched configuration
+REF_STRIDE = 8          # the CPU arms solve every REF_STRIDE-th system per step
+PLAIN_ITMAX = 400
 
 
 def peaks():
@@ -202,7 +206,7 @@ def run_reference(args, rank, world):
     threads = os.cpu_count() or 1
     vals = []
     cb = None
-    iters = args.ref_iters
+    iters = 69   # the solve's iteration count on this system (natural-order ILU(0))
     for s in range(args.warmup + args.steps):
         cb = cpu_baseline(J, B, iters, threads)
         if s >= args.warmup:
@@ -226,7 +230,346 @@ def workload_config(world):
             "parallelism": f"replicas x{world} (independent grids)"}
 
 
-def kernel_only(name, reps, iters=24, ordering="natural"):
+def traffic_record(name):
+    """DRAM bytes (read + write) per launch of a kernel on a workload, from the ncu capture
+    summarised in profiles/traffic.json (written with the command that produced it); None
+    when there is no capture of that kernel on that workload."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            rec = json.load(f).get(name)
+        return rec
+    except (OSError, ValueError):
+        return None
+
+
+def direct_error(A, B, X):
+    """||X - A \\ B||_F / ||A \\ B||_F with SciPy's sparse LU (FP64) as the direct solve."""
+    import numpy as np
+    import scipy.sparse.linalg as sla
+
+    Xd = sla.splu(A.tocsc(), permc_spec="COLAMD").solve(np.asarray(B, dtype=np.float64))
+    return float(np.linalg.norm(X - Xd) / np.linalg.norm(Xd))
+
+
+def rel_residual(A, B, X):
+    import numpy as np
+
+    return float(np.linalg.norm(B - A @ X) / np.linalg.norm(B))
+
+
+# ---- the batched configuration -----------------------------------------------------------
+def batch_sizes(nsys=NSYS, seed=0):
+    from blockpowerflow_b200 import grid as g
+
+    return g.batch_sizes(nsys, seed)
+
+
+def batch_workload(nsys=NSYS, seed=0, systems=None):
+    """The batched configuration's inputs (all systems, or the listed ones): grid.batch_workload."""
+    from blockpowerflow_b200 import grid as g
+
+    return g.batch_workload(nsys, seed, systems)
+
+
+def batch_config(nsys=NSYS):
+    """The workload, identical in both arms' lines."""
+    buses, nrhs = batch_sizes(nsys)
+    return {"workload": f"batch{nsys}_grids100-3000_p8-64", "systems": nsys,
+            "buses": "log-uniform 100-3000 per system (seeded)", "rhs_per_system": "U{8..64}",
+            "rhs_total": int(sum(nrhs)), "rhs": "Gaussian", "rtol": RTOL, "atol": 0.0,
+            "solver": "ILU0 block-GMRES (right preconditioner, ldiv), unrestarted",
+            "step": "ILU0 numeric factorization of every system + the solve of every right-hand side",
+            "l2": "inputs larger than L2 (blocks and bases of all systems), L2 flushed between steps",
+            "parallelism": "systems shared out over the ranks (LPT), no data-path collective"}
+
+
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    return O
+
+
+def cpu_batch_sample(mats, Bs, threads):
+    """The oracle's block-GMRES + natural-order FP64 ILU(0) (the reference's per-system call) on
+    the given systems, one system per host thread (longest first), cache-blocked dense products.
+    Returns (seconds, converged RHS, all solved)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    O = _oracle()
+    O.set_threads(1)
+    O.set_fast_dense(True)
+
+    def one(k):
+        A, B = mats[k], Bs[k]
+        X, st = O.block_gmres(A, B, N=(1, O.ilu0(A)), memory=PLAIN_ITMAX, restart=False, atol=0.0,
+                              rtol=RTOL, itmax=PLAIN_ITMAX)
+        return B.shape[1] if st.solved else 0, bool(st.solved)
+
+    order = sorted(range(len(mats)), key=lambda k: -mats[k].shape[0] * Bs[k].shape[1])
+    try:
+        t0 = time.time()
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            res = list(ex.map(one, order))
+        dt = time.time() - t0
+    finally:
+        O.set_fast_dense(False)
+    return dt, sum(r for r, _ in res), all(ok for _, ok in res)
+
+
+def run_reference_batch(args, rank, world):
+    """Reference arm: the C restatement of the reference CPU path on all host cores, each step
+    every REF_STRIDE-th system of the batch (offset by the step), same metric and config."""
+    if rank != 0:
+        return
+    buses, nrhs, mats, Bs = batch_workload()
+    threads = os.cpu_count() or 1
+    t_tot, rhs_tot, ok_all = 0.0, 0, True
+    for s in range(args.warmup + args.steps):
+        idx = list(range(s % REF_STRIDE, NSYS, REF_STRIDE))
+        dt, rhs, ok = cpu_batch_sample([mats[k] for k in idx], [Bs[k] for k in idx], threads)
+        if s >= args.warmup:
+            t_tot += dt
+            rhs_tot += rhs
+            ok_all = ok_all and ok
+    v = rhs_tot / t_tot
+    cb = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+          "sample": (f"every {REF_STRIDE}th system of the {NSYS} (offset = step), each step's "
+                     f"{NSYS // REF_STRIDE} systems one per host thread, oracle block-GMRES + FP64 "
+                     "natural-order ILU0 (the reference's per-system call), cache-blocked dense products"),
+          "all_solved": ok_all, "seconds": t_tot}
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_tot / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": batch_config(),
+            "method": "oracle (C restatement of block_gmres! + csrilu02-semantics ILU0), FP64, natural order",
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def headline_batch(args, rank, world, dist):
+    import numpy as np
+    import torch
+
+    import blockpowerflow_b200 as bpf
+    from blockpowerflow_b200 import replicas
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    buses, nrhs_all = batch_sizes()
+    # LPT share of the systems (all of them on one GPU); unknowns ~ 1.89 x buses
+    costs = [replicas.batch_system_cost(1.89 * b, p) for b, p in zip(buses, nrhs_all)]
+    mine = replicas.assign_systems(costs, world)[rank]
+    _, _, mats, Bs = batch_workload(systems=mine)
+    nrhs = [nrhs_all[k] for k in mine]
+    my_rhs = int(sum(nrhs))
+    dm = [bpf.CuSparseMatrixCSR.from_scipy(A, device=dev) for A in mats]
+    Bd = [bpf.colmajor(torch.as_tensor(B, device=dev)) for B in Bs]
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- set-up: autotuned launch shape, pattern analysis and graph capture ----
+    t0 = time.time()
+    tune = bpf.autotune(dm, nrhs, Bd, cache_path=os.environ.get("BPF_TUNE_CACHE"), repeats=1)
+    t_tune = time.time() - t0
+    t0 = time.time()
+    plan = bpf.BatchPlan(dm, nrhs, slice=tune["slice"], ctas_per_sm=tune["ctas_per_sm"])
+    torch.cuda.synchronize()
+    t_plan = time.time() - t0
+    Xd = [bpf.empty_colmajor(A.shape[0], p, dev) for A, p in zip(mats, nrhs)]
+    for _ in range(max(3, args.warmup)):
+        _, st = plan.solve(Bd, Xd)
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    # ---- timed region: K graph launches, instrumentation off ----
+    bpf._lib.set_timing(False)
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    l0 = bpf.kernel_launches()
+    barrier()
+    if sampler:
+        sampler.start()
+    ev, solved_rhs = [], 0
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, st = plan.solve(Bd, Xd)
+        e1.record()
+        ev.append((e0, e1))
+        solved_rhs += sum(p for p, s in zip(nrhs, st) if s.solved)
+    barrier()
+    clocks = sampler.stop() if sampler else None
+    launches = bpf.kernel_launches() - l0
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    tot_rhs, t_max = replicas.aggregate(solved_rhs, t_ms, device=dev)
+    value = tot_rhs / (t_max / 1e3)
+
+    # ---- checks outside the timed regions: true residuals and the direct-solve error ----
+    Xh = [X.cpu().numpy() for X in Xd]
+    rel = [rel_residual(A, B, X) for A, B, X in zip(mats, Bs, Xh)]
+    err = [direct_error(A, B, X) for A, B, X in zip(mats, Bs, Xh)]
+
+    # ---- instrumented pass (per-kernel CUDA events; not part of `value`) ----
+    units = plan.unit_stats()
+    cyc = plan.unit_cycles()
+    bpf._lib.set_timing(True)
+    for _ in range(2):
+        flush.fill_(1.0)
+        plan.solve(Bd, Xd)
+    torch.cuda.synchronize()
+    kern = _class_rates(bpf, ("factor", "batch"))
+    bpf._lib.set_timing(False)
+
+    # ---- end to end: pinned host B in, X out, through the public API ----
+    # host blocks p x n row-major = the column-major n x p blocks of the API
+    Bh = [torch.from_numpy(np.ascontiguousarray(B.T)).pin_memory() for B in Bs]
+    Xh_pin = [torch.empty((p, A.shape[0]), dtype=torch.float64).pin_memory() for A, p in zip(mats, nrhs)]
+    Bdev = [torch.empty((p, A.shape[0]), dtype=torch.float64, device=dev) for A, p in zip(mats, nrhs)]
+    h2d = int(sum(8 * B.size for B in Bs))
+
+    def step_e2e():
+        for bd, bh in zip(Bdev, Bh):
+            bd.copy_(bh, non_blocking=True)
+        _, s_ = plan.solve([bd.t() for bd in Bdev], Xd)
+        for xh, xd in zip(Xh_pin, Xd):
+            xh.copy_(xd.t(), non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return s_
+
+    for _ in range(2):
+        step_e2e()
+    barrier()
+    e_ms, e_rhs = 0.0, 0
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s_ = step_e2e()
+        e1.record()
+        torch.cuda.synchronize()
+        e_ms += e0.elapsed_time(e1)
+        e_rhs += sum(p for p, s in zip(nrhs, s_) if s.solved)
+    e_tot, e_max = replicas.aggregate(e_rhs, e_ms, device=dev)
+    Xe = [x.numpy().T for x in Xh_pin]
+    e2e_err = max(float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(Xe, Xh))
+
+    # ---- the plain FP64 drop-in on the same inputs: ilu0(A, p) + block_gmres per system ----
+    precs = [bpf.ilu0(A, p) for A, p in zip(dm, nrhs)]
+
+    def plain_pass():
+        out, ok = [], 0
+        for A, B, N, p in zip(dm, Bd, precs, nrhs):
+            N.refactor(A.nzVal)
+            X, s = bpf.block_gmres(A, B, N=N, ldiv=True, restart=False, memory=PLAIN_ITMAX, atol=0.0,
+                                   rtol=RTOL, itmax=PLAIN_ITMAX)
+            out.append((X, s))
+            ok += p if s.solved else 0
+        return out, ok
+
+    plain_pass()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    pres, p_rhs = plain_pass()
+    e1.record()
+    torch.cuda.synchronize()
+    p_ms = e0.elapsed_time(e1)
+    p_tot, p_max = replicas.aggregate(p_rhs, p_ms, device=dev)
+    plain_value = p_tot / (p_max / 1e3)
+    pX = [X.cpu().numpy() for X, _ in pres]
+    # per-system records of both paths, gathered once on rank 0 (the sharded batch's one gather)
+    recs = {k: {"niter": int(s_.niter), "solved": bool(s_.solved), "relres": r_, "err": e_,
+                "plain_niter": int(ps.niter), "plain_solved": bool(ps.solved),
+                "plain_relres": rel_residual(A, B, X), "plain_err": direct_error(A, B, X)}
+            for k, s_, r_, e_, (_, ps), A, B, X in zip(mine, st, rel, err, pres, mats, Bs, pX)}
+    del precs, pres
+    allrec = replicas.gather_to_root(recs)
+
+    # ---- CPU baseline (rank 0 at N = 1): every REF_STRIDE-th system on all host cores ----
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        idx = list(range(0, len(mats), REF_STRIDE))
+        dt, c_rhs, c_ok = cpu_batch_sample([mats[k] for k in idx], [Bs[k] for k in idx], threads)
+        cb = {"value": c_rhs / dt, "unit": UNIT, "cores": threads, "kind": "port",
+              "sample": (f"every {REF_STRIDE}th system of the {NSYS} ({len(idx)} systems, "
+                         f"{sum(nrhs[k] for k in idx)} RHS), one system per host thread, oracle block-GMRES "
+                         "+ FP64 natural-order ILU0, cache-blocked dense products"),
+              "seconds": dt, "all_solved": c_ok}
+
+    # ---- roofline of the persistent solve kernel ----
+    hbm, hbm_src = peaks()
+    kb = kern.get("batch", {})
+    k_launch_us = kb.get("avg_us")
+    k_bytes = kb.get("bytes_per_launch")
+    ach = (k_bytes / (k_launch_us / 1e6) / 1e9) if k_bytes and k_launch_us else None
+    cfg_all = batch_config()
+    traffic = traffic_record(f"batch_solve_kernel/{cfg_all['workload']}") if world == 1 else None
+    roofline = {"bound": "hbm", "kernel": "batch_solve_kernel (persistent block-GMRES of every unit)",
+                "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm if ach else None,
+                "peak_source": hbm_src, "avg_launch_us": k_launch_us, "bytes_per_launch": k_bytes,
+                "traffic": traffic["dram_bytes_per_launch"] if traffic else None,
+                "traffic_source": traffic["source"] if traffic else None,
+                "algorithmic_bytes": ("per unit iteration: ILU0 factors (4 + 4)(nnz_L + nnz_U) + 16(n+1) + 4n, "
+                                      "SpMM 12 nnz + 4(n+1), the new block 8 n q x 14 passes, plus "
+                                      "32 n q per basis block read (four CGS2 passes)")}
+    tot = {k: int(v.sum()) for k, v in cyc.items()}
+    plan.close()
+    if rank != 0:
+        return
+    assert sorted(allrec) == list(range(NSYS)), "every system solved exactly once"
+    R = [allrec[k] for k in range(NSYS)]
+    iters = [r["niter"] for r in R]
+    p_iters = [r["plain_niter"] for r in R]
+    all_ok = all(r["solved"] and r["relres"] <= RTOL * (1 + 1e-7) for r in R)
+    max_rel = max(r["relres"] for r in R)
+    max_err = max(r["err"] for r in R)
+    p_rel = max(r["plain_relres"] for r in R)
+    p_err = max(r["plain_err"] for r in R)
+    p_ok = all(r["plain_solved"] and r["plain_relres"] <= RTOL * (1 + 1e-7) for r in R)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": t_max / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64 (FP32 ILU0 factors)", "data": "synthetic", "config": cfg_all,
+        "method": {"value": "batched: one CUDA-graph launch per step (ILU0 kernel + persistent block-GMRES "
+                            "kernel), FP32 ILU0 factors in minimum-degree order, FP64 SpMM / orthogonalization / "
+                            "Hessenberg least squares / X, flexible GMRES, autotuned launch shape",
+                   "slice": tune["slice"], "ctas_per_sm": tune["ctas_per_sm"], "units": plan.nunits,
+                   "grid": plan.grid},
+        "all_solved": all_ok, "max_relres": max_rel,
+        "err_vs_direct": {"max": max_err, "median": float(np.median([r["err"] for r in R])),
+                          "how": "||X - splu(A) \\ B||_F / ||splu(A) \\ B||_F per system"},
+        "iterations": {"max": int(max(iters)), "mean": float(np.mean(iters))},
+        "plain_fp64_dropin": {"value": plain_value, "ms_per_step": p_max, "all_solved": p_ok,
+                              "max_relres": p_rel,
+                              "err_vs_direct": {"max": p_err,
+                                                "median": float(np.median([r["plain_err"] for r in R]))},
+                              "iterations": {"max": int(max(p_iters)), "mean": float(np.mean(p_iters))},
+                              "how": "ilu0(A, p) (FP64, natural order) at set-up; per step refactor + "
+                                     "block_gmres(A, B; N, ldiv=true, restart=false) per system, one after another"},
+        "batched_over_plain": value / plain_value,
+        "e2e": {"value": e_tot / (e_max / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(h2d), "max_rel_diff_vs_device_X": e2e_err},
+        "gpu_launches": int(launches), "roofline": roofline, "kernels": kern,
+        "phase_share": {k: round(v / max(tot["total"], 1), 4) for k, v in tot.items() if k != "total"},
+        "unit_cycles": {"max": int(cyc["total"].max()), "mean": float(cyc["total"].mean()),
+                        "balanced_bound_ms": float(cyc["total"].sum()) / plan.grid / 1.965e6,
+                        "critical_path_ms": float(cyc["total"].max()) / 1.965e6},
+        "autotune": {"seconds": t_tune, **{k: v for k, v in tune.items() if k != "cached"}},
+        "plan_seconds": t_plan, "systems_this_rank": len(mine), "rhs_this_rank": my_rhs,
+        "cpu_baseline": cb, "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def kernel_only(name, reps, iters=24, ordering="natural", nsys=64):
     """A few launches of one kernel on a case whose blocks exceed L2, for ncu captures:
     70,000-bus grid (134,998 unknowns, ~980k nonzeros), 128 right-hand sides."""
     import numpy as np
@@ -234,6 +577,23 @@ def kernel_only(name, reps, iters=24, ordering="natural"):
 
     import blockpowerflow_b200 as bpf
 
+    if name == "batch":
+        # `reps` solves of the first `nsys` systems of the batched configuration (the launch
+        # shape the autotuner picks for the full batch: slice 32, one CTA per SM); nsys = 512 is
+        # the whole batch
+        _, nrhs, mats, Bs = batch_workload(systems=range(nsys))
+        nrhs = nrhs[:nsys]
+        dm = [bpf.CuSparseMatrixCSR.from_scipy(A) for A in mats]
+        Bd = [bpf.colmajor(torch.as_tensor(B, device="cuda")) for B in Bs]
+        plan = bpf.BatchPlan(dm, nrhs, slice=32, ctas_per_sm=1)
+        for _ in range(reps):
+            Xs, st = plan.solve(Bd)
+        torch.cuda.synchronize()
+        print(json.dumps({"kernel_only": name, "systems": nsys, "rhs": int(sum(nrhs)), "reps": reps,
+                          "solved": all(s.solved for s in st), "units": plan.nunits,
+                          "device_bytes": plan.device_bytes}))
+        plan.close()
+        return
     if name == "gmres":
         # `iters` iterations of the benchmark's solve (9,000-bus grid, 64 RHS; 69 = the whole
         # solve): every kernel of the block-GMRES iteration, for a launch list
@@ -290,6 +650,7 @@ def _class_rates(bpf, classes):
         ms, cnt, by, fl = bpf._lib.kernel_time(kc)
         if cnt:
             out[kc] = {"ms": ms, "launches": cnt, "avg_us": 1e3 * ms / cnt,
+                       "bytes_per_launch": by / cnt, "flops_per_launch": fl / cnt,
                        "GBps": by / (ms / 1e3) / 1e9 if by and ms > 0 else None,
                        "TFLOPs": fl / (ms / 1e3) / 1e12 if fl and ms > 0 else None}
     return out
@@ -334,12 +695,17 @@ def config_rf25k(args):
     for t in range(max(3, args.warmup)):
         step(t)
     torch.cuda.synchronize()
-    # residual of every value set (outside the timed region)
-    worst = 0.0
+    # residual of every value set, and the error against SciPy's sparse LU on two of them
+    # (outside the timed region)
+    worst, err = 0.0, 0.0
     for t in range(nsets):
         step(t)
         R = bpf.mul(A, X, alpha=-1.0, beta=1.0, Y=Bd.clone())
         worst = max(worst, float(torch.linalg.norm(R) / torch.linalg.norm(Bd)))
+        if t < 2:
+            Jt = J.copy()
+            Jt.data = vals[t].copy()
+            err = max(err, direct_error(Jt, B, X.cpu().numpy()))
     steps = args.steps if args.steps > 5 else 100
     bpf._lib.set_timing(True)
     torch.cuda.synchronize()
@@ -369,6 +735,7 @@ def config_rf25k(args):
             "metric": "RHS solves/s (refactor + solve per step)", "unit": "RHS solves/s",
             "value": nrhs * steps / (t_ms / 1e3), "ms_per_step": t_ms / steps,
             "analyze_s": t_analyze, "max_relres": worst, "dtype": "f64",
+            "err_vs_direct": {"max": err, "how": "||X - splu(A_t) \\ B||_F / ||splu(A_t) \\ B||_F, value sets 0 and 1"},
             "kernels": kern,
             "roofline_sparse": {k: {"achieved_GBps": v["GBps"], "frac_of_hbm": v["GBps"] / hbm,
                                     "peak_source": hbm_src} for k, v in kern.items() if v["GBps"]},
@@ -425,6 +792,7 @@ def config_gmres300(args):
             "value": p * steps / (t_ms / 1e3), "ms_per_step": t_ms / steps, "iterations": st.niter,
             "oracle_iterations": so.niter, "relres": rel,
             "rel_diff_vs_oracle": float(np.linalg.norm(Xh - Xo) / np.linalg.norm(Xo)),
+            "err_vs_direct": direct_error(J, B, Xh),
             "dtype": "f64",
             "cpu_baseline": {"value": p / t_cpu, "unit": "RHS solves/s", "cores": 1, "kind": "port",
                              "sample": f"{reps} full solves"}}
@@ -456,7 +824,8 @@ def config_bicgstab9k(args):
         Xh = X.cpu().numpy()
         rel = float(np.linalg.norm(B - J @ Xh) / np.linalg.norm(B)) if np.all(np.isfinite(Xh)) else None
         out[name] = {"iterations": st.niter, "solved": bool(st.solved), "status": st.status,
-                     "relres": rel, "ms": e0.elapsed_time(e1)}
+                     "relres": rel, "ms": e0.elapsed_time(e1),
+                     "err_vs_direct": direct_error(J, B, Xh) if rel is not None else None}
     line = {"config": {"workload": "grid9k_p64_block_bicgstab_ilu0", "unknowns": n, "rhs": P_RHS,
                        "itmax": 400, "rtol": RTOL},
             "metric": "RHS solves/s at 1e-8 residual", "unit": "RHS solves/s",
@@ -539,6 +908,9 @@ def config_newton9k(args):
             "host_ms": 1e3 * cold[0] - dev_ms - asm_ms,
             "sensitivity_rel_diff_vs_superlu": float(np.linalg.norm(r.sensitivities - rc.sensitivities)
                                                      / np.linalg.norm(rc.sensitivities)),
+            "err_vs_direct": {"max": float(np.linalg.norm(r.sensitivities - rc.sensitivities)
+                                           / np.linalg.norm(rc.sensitivities)),
+                              "how": "sensitivities dx/du against the SciPy SuperLU loop's"},
             "cpu_baseline": {"value": t_cpu, "unit": "s", "cores": 1,
                              "kind": "numpy assembly + scipy SuperLU in the same loop",
                              "iterations": rc.iterations},
@@ -546,189 +918,14 @@ def config_newton9k(args):
     print(json.dumps(line), flush=True)
 
 
-def batch_workload(nsys=512, seed=0):
-    """Fourth configuration's inputs: nsys synthetic grids with log-uniform 100 - 3,000 buses
-    and U{8..64} Gaussian right-hand sides each (seeded)."""
-    import numpy as np
-
-    from blockpowerflow_b200 import grid as g
-
-    rng = np.random.default_rng(seed)
-    buses = np.exp(rng.uniform(np.log(100), np.log(3000), nsys)).astype(int)
-    nrhs = rng.integers(8, 65, nsys)
-    mats = [g.jacobian(g.make_grid(int(b), seed=1000 + k)).tocsr() for k, b in enumerate(buses)]
-    Bs = [g.gaussian_rhs(A.shape[0], int(p), 5000 + k) for k, (A, p) in enumerate(zip(mats, nrhs))]
-    return buses, [int(p) for p in nrhs], mats, Bs
-
-
-def config_batch512(args):
-    """Fourth configuration: 512 independent grids (100 - 3,000 buses, log-uniform), 8 - 64
-    RHS each, ILU(0) block-GMRES in one persistent CUDA-graph launch (FP32 factors, FP64
-    residual and orthogonalization), launch shape chosen by the autotuner.  One step = the
-    ILU(0) of every system + the solve of every right-hand side (one graph launch).  Beside it:
-    the plain FP64 drop-in (bpf.ilu0 + bpf.block_gmres per system, natural order, one system
-    after another) on the same inputs, and the oracle on a sample of the systems."""
-    import numpy as np
-    import torch
-
-    import blockpowerflow_b200 as bpf
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-
-    nsys = int(os.environ.get("BPF_BATCH_NSYS", "512"))
-    buses, nrhs, mats, Bs = batch_workload(nsys)
-    total_rhs = int(sum(nrhs))
-    dm = [bpf.CuSparseMatrixCSR.from_scipy(A) for A in mats]
-    Bd = [torch.as_tensor(B, device="cuda") for B in Bs]
-    t0 = time.time()
-    tune = bpf.autotune(dm, nrhs, Bd, cache_path=os.environ.get("BPF_TUNE_CACHE"), repeats=1)
-    t_tune = time.time() - t0
-    t0 = time.time()
-    plan = bpf.BatchPlan(dm, nrhs, slice=tune["slice"], ctas_per_sm=tune["ctas_per_sm"])
-    torch.cuda.synchronize()
-    t_plan = time.time() - t0
-    for _ in range(max(3, args.warmup)):
-        Xs, st = plan.solve(Bd)
-    torch.cuda.synchronize()
-    worst = 0.0
-    for A, B, X in zip(mats, Bs, Xs):
-        worst = max(worst, float(np.linalg.norm(B - A @ X.cpu().numpy()) / np.linalg.norm(B)))
-    solved = all(x.solved for x in st)
-    units = plan.unit_stats()
-    cyc = plan.unit_cycles()
-    steps = max(args.steps, 5)
-    launches0 = bpf.kernel_launches()
-    bpf._lib.set_timing(True)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(steps):
-        Xs, st = plan.solve(Bd)
-    e1.record()
-    torch.cuda.synchronize()
-    t_ms = e0.elapsed_time(e1)
-    launches = bpf.kernel_launches() - launches0
-    ms_b, cnt_b, by_b, fl_b = bpf._lib.kernel_time("batch")
-    bpf._lib.set_timing(False)
-    # end to end: host (pinned) B in, X out, through the public API
-    Bh = [torch.as_tensor(B).pin_memory() for B in Bs]
-    h2d = sum(B.numel() * 8 for B in Bh)
-    torch.cuda.synchronize()
-    te = time.time()
-    e_steps = max(2, steps // 2)
-    for _ in range(e_steps):
-        Xs_e, _ = plan.solve([B.to("cuda", non_blocking=True) for B in Bh])
-        Xh = [X.cpu() for X in Xs_e]
-    torch.cuda.synchronize()
-    t_e2e = (time.time() - te) / e_steps
-    # the plain FP64 drop-in, one system after another (natural-order ILU(0), unrestarted)
-    torch.cuda.synchronize()
-    tp = time.time()
-    plain_ok = True
-    for A, B, p in zip(dm, Bd, nrhs):
-        N = bpf.ilu0(A, p)
-        X, s = bpf.block_gmres(A, B, N=N, ldiv=True, restart=False, memory=400, atol=0.0, rtol=RTOL,
-                               itmax=400)
-        plain_ok = plain_ok and s.solved
-    torch.cuda.synchronize()
-    t_plain = time.time() - tp
-    # CPU: the oracle's block-GMRES on a sample of the systems (1 thread), scaled by RHS
-    O.set_threads(1)
-    O.set_fast_dense(True)   # cache-blocked dense products while timing
-    idx = list(range(0, nsys, max(1, nsys // 8)))[:8]
-    tc = time.time()
-    for k in idx:
-        O.block_gmres(mats[k], Bs[k], N=(1, O.ilu0(mats[k])), memory=400, restart=False, atol=0.0,
-                      rtol=RTOL, itmax=400)
-    t_cpu = time.time() - tc
-    O.set_fast_dense(False)
-    cpu_rhs = sum(nrhs[k] for k in idx)
-    hbm, hbm_src = peaks()
-    achieved = by_b / (ms_b / 1e3) / 1e9 if ms_b > 0 else None
-    tot = {k: int(v.sum()) for k, v in cyc.items()}
-    value = total_rhs * steps / (t_ms / 1e3)
-    line = {"config": {"workload": f"batch{nsys}_grids100-3000_p8-64", "systems": nsys,
-                       "unknowns_total": int(sum(A.shape[0] for A in mats)), "rhs_total": total_rhs,
-                       "nnz_total": int(sum(A.nnz for A in mats)), "units": plan.nunits,
-                       "grid": plan.grid, "slice": tune["slice"], "ctas_per_sm": tune["ctas_per_sm"],
-                       "ordering": "AMD (minimum degree)", "factors": "FP32", "rtol": RTOL,
-                       "l2": "inputs larger than L2 (all systems' bases)"},
-            "metric": "RHS solves/s at 1e-8 residual (batched)", "unit": "RHS solves/s",
-            "value": value, "ms_per_step": t_ms / steps, "steps": steps,
-            "all_solved": solved, "max_relres": worst,
-            "iterations": {"max": int(units["niter"].max()), "mean": float(units["niter"].mean())},
-            "phase_share": {k: round(v / max(tot["total"], 1), 4) for k, v in tot.items() if k != "total"},
-            "unit_cycles": {"max": int(cyc["total"].max()), "mean": float(cyc["total"].mean()),
-                            "sum": int(cyc["total"].sum()),
-                            "balanced_bound_ms": float(cyc["total"].sum()) / plan.grid / 1.965e6,
-                            "critical_path_ms": float(cyc["total"].max()) / 1.965e6},
-            "gpu_launches": launches,
-            "e2e": {"value": total_rhs / t_e2e, "unit": "RHS solves/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": h2d},
-            "plain_fp64_dropin": {"value": total_rhs / t_plain, "seconds": t_plain, "all_solved": plain_ok,
-                                  "how": "bpf.ilu0 + bpf.block_gmres per system, natural order"},
-            "batched_over_plain": value / (total_rhs / t_plain),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm if achieved else None, "peak_source": hbm_src,
-                         "kernel": "batch graph (factor + persistent solve)",
-                         "bytes_per_step": by_b / max(cnt_b, 1)},
-            "autotune": {"seconds": t_tune, **{k: v for k, v in tune.items() if k != "cached"}},
-            "plan_seconds": t_plan,
-            "cpu_baseline": {"value": cpu_rhs / t_cpu, "unit": "RHS solves/s", "cores": 1, "kind": "port",
-                             "sample": f"{len(idx)} of the {nsys} systems, full solves"},
-            "dtype": "f64 (FP32 factors)", "data": "synthetic"}
-    print(json.dumps(line), flush=True)
-
-
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel-only", choices=["trsv", "spmm", "factor", "gram", "gmres", "mlp"], default=None,
-                    help="launch one kernel a few times on a 135k-unknown case (for ncu)")
-    ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--iters", type=int, default=24, help="block-GMRES iterations (--kernel-only gmres)")
-    ap.add_argument("--ordering", default="natural", help="ILU(0) ordering (--kernel-only gmres)")
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ref-iters", type=int, default=69,
-                    help="iterations the reference arm extrapolates to (the GPU solve's count)")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", default="headline",
-                    choices=["headline", "gmres300", "bicgstab9k", "rf25k", "batch512", "newton9k"],
-                    help="the other benchmark configurations (one JSON line each, one GPU)")
-    args = ap.parse_args()
-    if args.config != "headline":
-        {"gmres300": config_gmres300, "bicgstab9k": config_bicgstab9k,
-         "rf25k": config_rf25k, "batch512": config_batch512, "newton9k": config_newton9k}[args.config](args)
-        return
-    if args.kernel_only:
-        kernel_only(args.kernel_only, args.reps, args.iters, args.ordering)
-        return
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+def config_gmres9k(args, rank, world, dist):
+    """The 9,000-bus grid of the second benchmark configuration (16,998 unknowns, ~121k nonzeros),
+    64 Gaussian right-hand sides, block-GMRES with a right ILU(0), no restart (as in
+    benchmarks_nvidia.jl), atol 0, rtol 1e-8.  One step = ILU(0) numeric refactorization + the
+    solve.  Variants: plain FP64 natural-order ILU(0) (the drop-in), FP32 factors,
+    minimum-degree order (FP64 / FP32 factors) and the learned warm start + rank-16 deflation.
+    Every rank solves its own grid (seed offset by rank)."""
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist_
-
-        dist = dist_
-        backend = "nccl" if args.impl == "ours" else "gloo"
-        if backend == "nccl":
-            import torch
-
-            torch.cuda.set_device(local)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
-    if args.impl == "reference":
-        run_reference(args, rank, world)
-        if dist:
-            dist.barrier()
-            dist.destroy_process_group()
-        return
-
     import numpy as np
     import torch
 
@@ -810,7 +1007,7 @@ def main():
         torch.cuda.synchronize()
         sampler = ClockSampler(torch.cuda.current_device()) if (rank == 0 and sample_clocks) else None
         l0 = bpf.kernel_launches()
-        bpf._lib.set_timing(True)
+        bpf._lib.set_timing(False)
         barrier()
         if sampler:
             sampler.start()
@@ -827,6 +1024,12 @@ def main():
         clocks = sampler.stop() if sampler else None
         launches = bpf.kernel_launches() - l0
         t_ms = sum(a.elapsed_time(b) for a, b in ev)
+        # instrumented pass (per-kernel CUDA events), separate from the timed steps
+        bpf._lib.set_timing(True)
+        for _ in range(2):
+            flush.fill_(1.0)
+            solve(N)
+        torch.cuda.synchronize()
         kern = {}
         for kc in ("spmm", "trsv", "factor", "gram", "tsmm", "small", "chol", "hess", "backsub", "mlp"):
             ms, cnt, by, fl = bpf._lib.kernel_time(kc)
@@ -834,14 +1037,20 @@ def main():
         bpf._lib.set_timing(False)
         tot_rhs, t_max = replicas.aggregate(solved_rhs, t_ms, device=dev)
         value = tot_rhs / (t_max / 1e3)
-        R = B - J @ X.cpu().numpy()
+        Xn = X.cpu().numpy()
+        R = B - J @ Xn
         col_rel = np.linalg.norm(R, axis=0) / np.linalg.norm(B, axis=0)
         return {"value": value, "t_ms": t_ms, "t_max": t_max, "iterations": st.niter,
+                "err_vs_direct": float(np.linalg.norm(Xn - X_direct) / np.linalg.norm(X_direct)),
+                "instrumented_steps": 2,
                 "solved_fraction": solved_rhs / (P_RHS * args.steps),
                 "relres": float(np.linalg.norm(R) / np.linalg.norm(B)),
                 "max_column_relres": float(col_rel.max()), "launches": int(launches),
                 "kern": kern, "clocks": clocks}
 
+    import scipy.sparse.linalg as sla
+
+    X_direct = sla.splu(J.tocsc(), permc_spec="COLAMD").solve(B)
     results = {name: timed(name, name == "fp64") for name in variants}
     ok = {k: r for k, r in results.items() if r["solved_fraction"] == 1.0 and r["relres"] <= RTOL}
     head = max(ok, key=lambda k: ok[k]["value"]) if ok else "fp64"
@@ -870,7 +1079,8 @@ def main():
 
     # ---- roofline of the dominant kernel class -------------------------------------------
     hbm, hbm_src = peaks()
-    kern, t_ms = r["kern"], r["t_ms"]
+    kern = r["kern"]
+    t_ms = sum(v["ms"] for k, v in kern.items() if k != "hess")   # main-stream device time of the instrumented steps
     breakdown = {}
     for k, v in kern.items():
         if v["launches"] == 0:
@@ -900,7 +1110,7 @@ def main():
                     "frac": ach / hbm, "peak_source": hbm_src,
                     "bytes_per_launch": v["bytes"] / max(v["launches"], 1)}
     roofline.update({"avg_launch_us": 1e3 * v["ms"] / max(v["launches"], 1),
-                     "traffic": TRAFFIC_PER_LAUNCH.get(dom),
+                     "traffic": (traffic_record(f"{dom}/grid9k_p64_{head}") or {}).get("dram_bytes_per_launch"),
                      "dominant_share_of_device_time": v["ms"] / max(t_ms, 1e-9)})
     # the HBM-bound sparse kernels beside it (triangular solves, SpMM)
     sparse = {}
@@ -913,7 +1123,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(J, B, results["fp64"]["iterations"], os.cpu_count() or 1)
     cfg = workload_config(world)
-    cfg["variant"] = {"fp64": "plain FP64 ILU0 (natural order)",
+    method = {"fp64": "plain FP64 ILU0 (natural order)",
                       "mixed": "FP32 ILU0 factors, flexible GMRES",
                       "amd": "minimum-degree-ordered FP64 ILU0",
                       "amd_mixed": "minimum-degree-ordered FP32 ILU0 factors, flexible GMRES",
@@ -922,10 +1132,12 @@ def main():
         "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": r["t_max"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": cfg,
+        "data": "synthetic", "config": cfg, "method": method,
         "iterations": iters, "relres": r["relres"], "max_column_relres": r["max_column_relres"],
+        "err_vs_direct": r["err_vs_direct"],
         "solved_fraction": r["solved_fraction"],
         "variants": {k: {"value": x["value"], "iterations": x["iterations"], "relres": x["relres"],
+                         "err_vs_direct": x["err_vs_direct"],
                          "solved_fraction": x["solved_fraction"], "ms_per_step": x["t_max"] / args.steps}
                      for k, x in results.items()},
         "mixed_over_plain_fp64": results["mixed"]["value"] / max(results["fp64"]["value"], 1e-30),
@@ -943,9 +1155,62 @@ def main():
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--kernel-only", choices=["trsv", "spmm", "factor", "gram", "gmres", "mlp", "batch"],
+                    default=None, help="launch one kernel a few times on a small case (for ncu)")
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--iters", type=int, default=24, help="block-GMRES iterations (--kernel-only gmres)")
+    ap.add_argument("--ordering", default="natural", help="ILU(0) ordering (--kernel-only gmres)")
+    ap.add_argument("--nsys", type=int, default=64, help="systems of the batch (--kernel-only batch)")
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", default="batch512",
+                    choices=["batch512", "gmres9k", "gmres300", "bicgstab9k", "rf25k", "newton9k"],
+                    help="batch512 (default): the batched configuration; the others print one line "
+                         "each for the other benchmark configurations")
+    args = ap.parse_args()
+    if args.kernel_only:
+        kernel_only(args.kernel_only, args.reps, args.iters, args.ordering, args.nsys)
+        return
+    if args.config in ("gmres300", "bicgstab9k", "rf25k", "newton9k"):
+        {"gmres300": config_gmres300, "bicgstab9k": config_bicgstab9k,
+         "rf25k": config_rf25k, "newton9k": config_newton9k}[args.config](args)
+        return
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_
+
+        dist = dist_
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    try:
+        if args.impl == "reference":
+            (run_reference_batch if args.config == "batch512" else run_reference)(args, rank, world)
+        elif args.config == "batch512":
+            headline_batch(args, rank, world, dist)
+        else:
+            config_gmres9k(args, rank, world, dist)
+    finally:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -84,6 +84,8 @@ SIGNATURES = {
     "bpf_solve_status_string": (C.c_char_p, [_I]),
     "bpf_ctx_kernel_launches": (C.c_longlong, [_P]),
     "bpf_ctx_set_timing": (_I, [_P, _I]),
+    "bpf_ctx_set_wait_limit": (_I, [_P, C.c_longlong]),
+    "bpf_selftest_grid_barrier": (_I, [_P, _I, _I, C.POINTER(_I)]),
     "bpf_ctx_kernel_time": (_I, [_P, _I, C.POINTER(_D), C.POINTER(C.c_longlong),
                                  C.POINTER(_D), C.POINTER(_D)]),
     "bpf_spmm": (_I, [_P, C.POINTER(CsrDesc), _I, _D, _P, _I, _D, _P, _I]),

@@ -192,3 +192,33 @@ def jacobian_on_pattern(grid: Grid, pattern: sp.csr_matrix, vm, va) -> np.ndarra
         raise ValueError("perturbed Jacobian left the fixed sparsity pattern")
     out[pos] = Jt.data
     return out
+
+
+# ---- the batched benchmark configuration: many independent grids of uneven size ----------
+def batch_sizes(nsys: int = 512, seed: int = 0):
+    """Bus counts (log-uniform in [100, 3000]) and right-hand-side counts (uniform in 8..64)
+    of a batch of ``nsys`` independent grids."""
+    rng = np.random.default_rng(seed)
+    buses = np.exp(rng.uniform(np.log(100), np.log(3000), nsys)).astype(int)
+    nrhs = rng.integers(8, 65, nsys)
+    return [int(b) for b in buses], [int(p) for p in nrhs]
+
+
+def batch_system(k: int, buses, nrhs):
+    """System ``k`` of a batch: its Jacobian (sorted CSR) and Gaussian right-hand sides."""
+    A = jacobian(make_grid(buses[k], seed=1000 + k)).tocsr()
+    B = gaussian_rhs(A.shape[0], nrhs[k], 5000 + k)
+    return A, B
+
+
+def batch_workload(nsys: int = 512, seed: int = 0, systems=None):
+    """(buses, nrhs, matrices, right-hand sides) of a batch, for all systems or the listed ones
+    (``buses`` and ``nrhs`` always cover the whole batch)."""
+    buses, nrhs = batch_sizes(nsys, seed)
+    idx = range(nsys) if systems is None else systems
+    mats, Bs = [], []
+    for k in idx:
+        A, B = batch_system(k, buses, nrhs)
+        mats.append(A)
+        Bs.append(B)
+    return buses, nrhs, mats, Bs

@@ -19,6 +19,19 @@ def solve_cost(n: int, nnz: int, p: int, iters: int = 50) -> float:
     return iters * 3.0 * nnz * p + 8.0 * n * p * p * iters * (iters + 1) / 2.0
 
 
+def batch_system_cost(n: int, p: int, qmax: int = 32) -> float:
+    """Cost model of one system of a batched solve (the plan's own unit estimate): p columns
+    in ceil(p / qmax) slices of width q, each ~1.5 (n / q)^0.7 iterations whose basis traffic
+    grows like iterations^2 n q."""
+    ns = max(1, -(-int(p) // int(qmax)))
+    cost = 0.0
+    for k in range(ns):
+        q = p // ns + (1 if k < p % ns else 0)
+        it = 1.5 * (float(n) / q) ** 0.7
+        cost += it * it * float(n) * q
+    return cost
+
+
 def assign_systems(costs, world: int):
     """Longest-processing-time-first assignment of systems to `world` ranks.
 
@@ -36,6 +49,39 @@ def assign_systems(costs, world: int):
     for lst in out:
         lst.sort()
     return out
+
+
+def allreduce_max(value: float, group=None, device=None) -> float:
+    """Max of a scalar over the ranks (the value itself without a process group)."""
+    import torch
+    import torch.distributed as dist
+
+    if not dist.is_available() or not dist.is_initialized():
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t.item())
+
+
+def gather_to_root(local: dict, group=None):
+    """Every rank's {system index: result} merged on rank 0 (None on the other ranks): the one
+    gather at the end of a sharded batch.  Without a process group, the local dict itself."""
+    import torch.distributed as dist
+
+    if not dist.is_available() or not dist.is_initialized():
+        return dict(local)
+    world = dist.get_world_size(group)
+    out = [None] * world if dist.get_rank(group) == 0 else None
+    dist.gather_object(local, out, dst=0, group=group)
+    if out is None:
+        return None
+    merged = {}
+    for part in out:
+        for k, v in part.items():
+            if k in merged:
+                raise ValueError(f"system {k} solved on two ranks")
+            merged[k] = v
+    return merged
 
 
 def aggregate(local_rhs: float, local_ms: float, group=None, device=None):

@@ -1,6 +1,7 @@
 // C ABI: context, errors, workspace, SpMM and preconditioner entry points.
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <vector>
 
@@ -64,7 +65,8 @@ cudaEvent_t timing_event(bpf_ctx *ctx) {
 }
 
 bpf_status reset_dev_status(bpf_ctx *ctx) {
-    BPF_CUDA(ctx, cudaMemsetAsync(ctx->dstat, 0, sizeof(DevStatus), ctx->stream));
+    // the error word and the barrier state; the wait limit stays as the caller set it
+    BPF_CUDA(ctx, cudaMemsetAsync(ctx->dstat, 0, offsetof(DevStatus, wait_limit), ctx->stream));
     return BPF_SUCCESS;
 }
 
@@ -256,6 +258,19 @@ bpf_status prec_setup(bpf_ctx *ctx, int kind, int n, const std::vector<int> &rp,
     return BPF_SUCCESS;
 }
 
+// Self-test of the bounded grid barrier: every block except `absent` (-1: none) meets at
+// one grid barrier; if a block never arrives the others give up after the context's wait limit,
+// record DEV_BARRIER_TIMEOUT and return.  `arrived` counts the blocks that passed the barrier.
+__global__ void barrier_selftest_kernel(DevStatus *ds, int absent, int *arrived) {
+    __shared__ unsigned s_gen;
+    if (threadIdx.x == 0) s_gen = barrier_gen_start(ds);
+    __syncthreads();
+    unsigned gen = s_gen;
+    if ((int)blockIdx.x == absent) return;
+    if (!grid_barrier(ds, gen)) return;
+    if (threadIdx.x == 0) atomicAdd(arrived, 1);
+}
+
 }  // namespace bpf
 
 using namespace bpf;
@@ -286,6 +301,7 @@ bpf_status bpf_ctx_create(bpf_ctx **out, void *stream) {
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_b[i], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) noalloc_forget_device(ctx->device);
     if (e != cudaSuccess) {
         cudaGetLastError();
         for (int i = 0; i < 2; i++) {
@@ -332,6 +348,41 @@ const char *bpf_last_error(const bpf_ctx *ctx) {
 }
 
 long long bpf_ctx_kernel_launches(const bpf_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+bpf_status bpf_ctx_set_wait_limit(bpf_ctx *ctx, long long polls) {
+    if (!ctx) return BPF_ERR_INVALID_VALUE;
+    if (polls < 0) return set_error(ctx, BPF_ERR_INVALID_VALUE, "wait limit must be >= 0");
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->hstat->wait_limit = polls;
+    BPF_CUDA(ctx, cudaMemcpyAsync(&ctx->dstat->wait_limit, &ctx->hstat->wait_limit, sizeof(long long),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return BPF_SUCCESS;
+}
+
+bpf_status bpf_selftest_grid_barrier(bpf_ctx *ctx, int nblocks, int absent_block, int *arrived) {
+    if (!ctx) return BPF_ERR_INVALID_VALUE;
+    if (nblocks < 2 || absent_block < -1 || absent_block >= nblocks)
+        return set_error(ctx, BPF_ERR_INVALID_VALUE, "selftest: nblocks >= 2 and -1 <= absent_block < nblocks");
+    int per_sm = 0;
+    BPF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, barrier_selftest_kernel, 128, 0));
+    if (nblocks > per_sm * ctx->num_sms)
+        return set_error(ctx, BPF_ERR_INVALID_VALUE, "selftest: at most %d co-resident blocks", per_sm * ctx->num_sms);
+    bpf_status st = BPF_SUCCESS;
+    int *d_arrived = (int *)ws_get(ctx, WS_SMALL, sizeof(int), &st);
+    if (!d_arrived) return st;
+    BPF_CUDA(ctx, cudaMemsetAsync(d_arrived, 0, sizeof(int), ctx->stream));
+    DevStatus *ds = ctx->dstat;
+    void *args[] = {&ds, &absent_block, &d_arrived};
+    BPF_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)barrier_selftest_kernel, dim3(nblocks), dim3(128),
+                                              args, 0, ctx->stream));
+    BPF_LAUNCHED(ctx);
+    int h = 0;
+    BPF_CUDA(ctx, cudaMemcpyAsync(&h, d_arrived, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    st = check_dev_status(ctx, "selftest_grid_barrier");   // synchronizes the stream
+    if (arrived) *arrived = h;
+    return st;
+}
 
 bpf_status bpf_ctx_set_timing(bpf_ctx *ctx, int on) {
     if (!ctx) return BPF_ERR_INVALID_VALUE;

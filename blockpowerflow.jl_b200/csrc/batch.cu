@@ -1036,6 +1036,10 @@ struct bpf_batch {
     cudaGraphExec_t gexec = nullptr;
     std::vector<double> unit_iter_bytes;   // algorithmic bytes of one iteration (without basis reads)
     std::vector<double> unit_basis_bytes;  // basis bytes per block read by one iteration
+    double factor_bytes = 0.0;             // algorithmic bytes of one launch of the factor kernel
+    double factor_flops = 0.0;
+    int factor_grid = 0;
+    Cfg cfg{};
 };
 
 namespace {
@@ -1206,6 +1210,12 @@ bpf_status bpf_batch_plan(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A, const i
         f.u_dinvf = pk.reserve(sizeof(float) * n);
         f.lnlev = L.nlev;
         f.unlev = U.nlev;
+        // factor kernel, per system: values in (8 + 4 map) and scattered twice (16), the update
+        // pairs' indices (8 each), the level-sorted FP64 + FP32 copies (map 4 + read 8 + 12 written)
+        // and the inverted diagonal
+        b->factor_bytes += 28.0 * nnz + 4.0 * (n + 1) + 8.0 * (double)pdst.size() +
+                           24.0 * ((double)f.lnnz + f.unnz) + 16.0 * n;
+        b->factor_flops += 2.0 * (double)pdst.size();
         b->n[s] = n;
         b->p[s] = nrhs[s];
         vals[s] = D.vals;
@@ -1371,11 +1381,13 @@ bpf_status bpf_batch_plan(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A, const i
     cfg.rtol = o.rtol;
     cfg.itmax = o.itmax;
     cfg.f32 = o.factor_dtype == BPF_F32;
+    b->cfg = cfg;
+    b->factor_grid = std::min(nsys, 4 * ctx->num_sms);
     cudaError_t e = cudaStreamBeginCapture(b->cstream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_io, b->h_io, sizeof(IO) * nsys, cudaMemcpyHostToDevice, b->cstream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->cstream);
     if (e == cudaSuccess) {
-        batch_factor_kernel<<<std::min(nsys, 4 * ctx->num_sms), kT, 0, b->cstream>>>(b->d_sys, nsys, b->d_err);
+        batch_factor_kernel<<<b->factor_grid, kT, 0, b->cstream>>>(b->d_sys, nsys, b->d_err);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
@@ -1406,9 +1418,25 @@ bpf_status bpf_batch_solve(bpf_batch *b, const double *const *B, const int *ldb,
         b->h_io[s].ldb = lb;
         b->h_io[s].ldx = lx;
     }
-    {
-        KScope ks(ctx, BPF_KC_BATCH, 0.0, 0.0);
+    if (!ctx->timing) {
         BPF_CUDA(ctx, cudaGraphLaunch(b->gexec, ctx->stream));
+        ctx->launches += 2;
+    } else {
+        // Per-kernel timing: the graph's four steps issued one by one on the context's stream,
+        // so that each kernel gets its own pair of events (same kernels, same arguments).
+        BPF_CUDA(ctx, cudaMemcpyAsync(b->d_io, b->h_io, sizeof(IO) * b->nsys, cudaMemcpyHostToDevice, ctx->stream));
+        BPF_CUDA(ctx, cudaMemsetAsync(b->d_counter, 0, sizeof(int), ctx->stream));
+        {
+            KScope ks(ctx, BPF_KC_FACTOR, b->factor_bytes, b->factor_flops);
+            batch_factor_kernel<<<b->factor_grid, kT, 0, ctx->stream>>>(b->d_sys, b->nsys, b->d_err);
+            BPF_CUDA(ctx, cudaGetLastError());
+        }
+        {
+            KScope ks(ctx, BPF_KC_BATCH, 0.0, 0.0);
+            batch_solve_kernel<<<b->grid, kT, smem_bytes(), ctx->stream>>>(b->d_sys, b->d_units, b->nunits, b->d_io,
+                                                                          b->d_err, b->cfg, b->d_out, b->d_counter);
+            BPF_CUDA(ctx, cudaGetLastError());
+        }
         ctx->launches += 2;
     }
     BPF_CUDA(ctx, cudaMemcpyAsync(b->h_out, b->d_out, sizeof(UnitOut) * b->nunits, cudaMemcpyDeviceToHost, ctx->stream));

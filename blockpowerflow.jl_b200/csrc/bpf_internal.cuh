@@ -29,7 +29,8 @@ struct DevStatus {
     int aux;        // row / column index for diagnostics
     unsigned bar_count;  // grid barrier arrival counter
     unsigned bar_gen;    // grid barrier generation
-    int pad[4];
+    long long wait_limit;  // polls before a grid barrier gives up (<= 0: kSpinLimit); kept by resets
+    int pad[2];
 };
 
 // Workspace slots held by a context (grow-only, reused across calls).
@@ -99,6 +100,9 @@ namespace bpf {
 // host-side error helpers
 // ------------------------------------------------------------------------------------
 bpf_status set_error(bpf_ctx *ctx, bpf_status st, const char *fmt, ...);
+// A library context was created on `dev`: bpf_prec_apply_noalloc looks its static scratch's
+// address up again on its next call there (noalloc.cu).
+void noalloc_forget_device(int dev);
 bpf_status cuda_error(bpf_ctx *ctx, cudaError_t e, const char *what, const char *file, int line);
 void *ws_get(bpf_ctx *ctx, int slot, size_t bytes, bpf_status *st);
 bpf_status check_dev_status(bpf_ctx *ctx, const char *where);
@@ -197,7 +201,8 @@ constexpr long long kSpinLimit = 1LL << 21;
 // Grid-wide barrier for a cooperative (co-resident) launch.  `gen` is the generation the
 // calling block last saw (read once at kernel start by thread 0 of each block).  Returns
 // false (in every thread of the block) if the barrier timed out or an error is pending, in
-// which case the caller must return without further global writes.
+// which case the caller must return without further global writes.  A waiting block gives up
+// after the context's wait limit (ds->wait_limit polls, kSpinLimit when not set).
 __device__ __forceinline__ bool grid_barrier(DevStatus *ds, unsigned &gen) {
     __shared__ int s_ok;
     __syncthreads();
@@ -215,8 +220,9 @@ __device__ __forceinline__ bool grid_barrier(DevStatus *ds, unsigned &gen) {
             st_release_u32(&ds->bar_gen, g + 1);
         } else {
             long long it = 0;
+            const long long lim = ds->wait_limit > 0 ? ds->wait_limit : kSpinLimit;
             while (ld_acquire_u32(&ds->bar_gen) == g) {
-                if (++it > kSpinLimit || ld_relaxed_i32(&ds->err) != 0) {
+                if (++it > lim || ld_relaxed_i32(&ds->err) != 0) {
                     ok = 0;
                     atomicCAS(&ds->err, 0, (int)DEV_BARRIER_TIMEOUT);
                     break;

@@ -127,6 +127,19 @@ BPF_API const char *bpf_solve_status_string(int status);
 /* Number of kernels this library launched on the context (a running counter). */
 BPF_API long long bpf_ctx_kernel_launches(const bpf_ctx *ctx);
 
+/* Failure detection.  Every cross-block wait of the library's kernels (the grid barriers of the
+ * cooperative triangular solves and factorizations) gives up after a bounded number of polls,
+ * records the timeout and returns, so a block that never arrives ends the call with
+ * BPF_ERR_TIMEOUT and leaves the context usable.  No counterpart in the reference, whose
+ * library calls block until the device finishes.  polls = 0 restores the default (~2^21 polls,
+ * about a second); smaller limits shorten the watchdog. */
+BPF_API bpf_status bpf_ctx_set_wait_limit(bpf_ctx *ctx, long long polls);
+/* Self-test of that path: a cooperative launch of nblocks (2.. co-resident maximum) blocks that
+ * meet at one grid barrier, block absent_block (-1: none) skipping it.  Returns BPF_SUCCESS when
+ * every block passed, BPF_ERR_TIMEOUT when the others gave up waiting for the absent one;
+ * *arrived (host, nullable) = the blocks that passed the barrier. */
+BPF_API bpf_status bpf_selftest_grid_barrier(bpf_ctx *ctx, int nblocks, int absent_block, int *arrived);
+
 /* Per-kernel-class device timing (CUDA events recorded around each launch on the context's
  * stream).  No counterpart in the reference: it stands in for the CUDA.@time / @time
  * measurements of test/*.jl and is what the benchmark uses to put a launch-averaged kernel
@@ -142,7 +155,7 @@ typedef enum {
     BPF_KC_HESS = 7,    /* block Hessenberg QR update (apply + factor) */
     BPF_KC_BACKSUB = 8, /* block back substitution of block-GMRES     */
     BPF_KC_MLP = 9,     /* learned warm start: tensor-core GEMMs       */
-    BPF_KC_BATCH = 10,  /* batched solve: factor + persistent solve graph */
+    BPF_KC_BATCH = 10,  /* batched solve: the persistent solve kernel (its ILU(0) kernel counts as FACTOR) */
     BPF_KC_PF = 11,     /* power-flow mismatch and Jacobian assembly  */
     BPF_KC_COUNT = 12
 } bpf_kernel_class;
@@ -245,12 +258,15 @@ BPF_API bpf_status bpf_prec_refactor(bpf_prec *prec, const double *vals);
 BPF_API bpf_status bpf_prec_apply(bpf_prec *prec, int p, const double *X, int ldx, double *Y,
                                   int ldy);
 /* No counterpart in the reference.  The same Y = P \ X as bpf_prec_apply for callers that
- * cannot allocate device memory once the preconditioner exists (code inside a stream capture,
- * hosts whose device memory belongs to an external pool or a fixed start-up arena, loops that
- * forbid allocation): its scratch is a static 8 MiB device array instead of a cudaMalloc'd
- * workspace.  Limit: n * min(p, 256) <= 1,048,576 doubles, else BPF_ERR_NOT_SUPPORTED.  All calls
- * on a device share the array (calls that overlap on the GPU race); the first call on a device
- * looks its address up and should come before any stream capture. */
+ * cannot allocate device memory once the preconditioner exists: hosts whose device memory
+ * belongs to an external pool or a fixed start-up arena (a cudaMalloc behind the pool's back can
+ * fail or fragment it) and real-time loops that forbid allocation after set-up (a cudaMalloc
+ * synchronizes the device and takes an unbounded time).  Its scratch is a static 8 MiB device
+ * array instead of a cudaMalloc'd workspace.  Limit: n * min(p, 256) <= 1,048,576 doubles, else
+ * BPF_ERR_NOT_SUPPORTED; a reordered preconditioner also takes at most the nrhs it was created
+ * for per 256-column slice (its own scratch is never grown here).  All calls on a device share
+ * the array and it keeps the last call's contents (calls that overlap on the GPU race); the
+ * first call on a device after a context was created there looks the array's address up. */
 BPF_API bpf_status bpf_prec_apply_noalloc(bpf_prec *prec, int p, const double *X, int ldx,
                                           double *Y, int ldy);
 /* Copy the factor values (A's pattern, nnz doubles, device pointer) out: the P field of

@@ -1,0 +1,117 @@
+"""Parity at the benchmark configurations' own sizes, against the FP64 direct solve.
+
+Each test compares the CUDA path (through the C ABI) with SciPy's sparse LU, not with this
+library itself:
+  * the 9,000-bus grid (16,998 unknowns), 64 right-hand sides, block-GMRES + FP64 natural-order
+    ILU(0): at the benchmark tolerance (rtol 1e-8) the true residual meets it; solved to rtol
+    1e-13, X agrees with the direct solve to 1e-10 (relative, Frobenius);
+  * the 25,000-bus grid (47,998 unknowns), 256 right-hand sides, three steps of the RF
+    sequence (analyse once, refactor on perturbed values, solve): X to 1e-10 of the direct solve
+    of each step's matrix (the reference's own check is isapprox at sqrt(eps),
+    test/cusolverRF.jl:21);
+  * all 512 systems of the batched configuration: FP32 factors, every system's true residual
+    <= 1e-8; FP64 factors solved to rtol 1e-13, every X within 1e-10 of the direct solve.
+"""
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def bpf():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import blockpowerflow_b200 as bpf
+
+    return bpf
+
+
+def _direct(A, B):
+    return spla.splu(A.tocsc(), permc_spec="COLAMD").solve(np.asarray(B))
+
+
+def _rel(X, Xd):
+    return float(np.linalg.norm(X - Xd) / np.linalg.norm(Xd))
+
+
+def test_grid9k_p64_block_gmres_ilu0_against_direct(bpf):
+    import torch
+
+    g = bpf.grid
+    J = g.jacobian(g.make_grid(9000, 1000, seed=0))
+    B = g.gaussian_rhs(J.shape[0], 64, 1000)
+    Xd = _direct(J, B)
+    A = bpf.CuSparseMatrixCSR.from_scipy(J)
+    Bt = torch.as_tensor(B, device="cuda")
+    N = bpf.ilu0(A, 64)
+    X, st = bpf.block_gmres(A, Bt, N=N, ldiv=True, restart=False, memory=300, atol=0.0, rtol=1e-8,
+                            itmax=300)
+    Xh = X.cpu().numpy()
+    assert st.solved
+    assert np.linalg.norm(B - J @ Xh) / np.linalg.norm(B) <= 1e-8
+    X, st = bpf.block_gmres(A, Bt, N=N, ldiv=True, restart=False, memory=300, atol=0.0, rtol=1e-13,
+                            itmax=300)
+    assert st.solved, st
+    assert _rel(X.cpu().numpy(), Xd) <= 1e-10
+
+
+def test_grid25k_rf_sequence_against_direct(bpf):
+    import torch
+
+    g = bpf.grid
+    RF = bpf.CUSOLVERRF
+    gr = g.make_grid(25000, 2000, seed=0)
+    J = g.jacobian(gr)
+    n = J.shape[0]
+    B = g.gaussian_rhs(n, 256, 1)
+    A = bpf.CuSparseMatrixCSR.from_scipy(J)
+    rf = RF.CusolverRfLU(A, nrhs=256, ordering="AMD")
+    Bt = torch.as_tensor(B, device="cuda")
+    for t in range(3):
+        vals = g.perturbed_values(gr, J, t, sigma=0.01, seed=0)
+        A.nzVal.copy_(torch.as_tensor(vals, device="cuda"))
+        RF.update_(rf, A)
+        X = bpf.colmajor(Bt.clone())
+        RF.ldiv_(rf, X)
+        Jt = J.copy()
+        Jt.data = vals.copy()
+        assert _rel(X.cpu().numpy(), _direct(Jt, B)) <= 1e-10, t
+
+
+@pytest.fixture(scope="module")
+def batch512(bpf):
+    return bpf.grid.batch_workload(512)
+
+
+def _batch_solve(bpf, mats, Bs, nrhs, **kw):
+    import torch
+
+    dm = [bpf.CuSparseMatrixCSR.from_scipy(A) for A in mats]
+    plan = bpf.BatchPlan(dm, nrhs, slice=32, ctas_per_sm=1, **kw)
+    try:
+        Xs, st = plan.solve([torch.as_tensor(B, device="cuda") for B in Bs])
+        return [X.cpu().numpy() for X in Xs], st
+    finally:
+        plan.close()
+
+
+def test_batch512_fp32_factors_every_system_meets_the_tolerance(bpf, batch512):
+    _, nrhs, mats, Bs = batch512
+    Xs, st = _batch_solve(bpf, mats, Bs, nrhs)
+    for s, (A, B, X) in enumerate(zip(mats, Bs, Xs)):
+        assert st[s].solved, (s, st[s])
+        assert np.linalg.norm(B - A @ X) / np.linalg.norm(B) <= 1e-8 * (1 + 1e-9), s
+
+
+def test_batch512_fp64_factors_match_the_direct_solve(bpf, batch512):
+    _, nrhs, mats, Bs = batch512
+    Xs, st = _batch_solve(bpf, mats, Bs, nrhs, factor_dtype="float64", rtol=1e-13)
+    worst = 0.0
+    for s, (A, B, X) in enumerate(zip(mats, Bs, Xs)):
+        assert st[s].solved, (s, st[s])
+        worst = max(worst, _rel(X, _direct(A, B)))
+    assert worst <= 1e-10, worst
