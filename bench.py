@@ -569,7 +569,7 @@ def headline_batch(args, rank, world, dist):
     print(json.dumps(line), flush=True)
 
 
-def kernel_only(name, reps, iters=24, ordering="natural", nsys=64):
+def kernel_only(name, reps, iters=24, ordering="natural", nsys=64, kgrid="case70k", kp=128, timed=False):
     """A few launches of one kernel on a case whose blocks exceed L2, for ncu captures:
     70,000-bus grid (134,998 unknowns, ~980k nonzeros), 128 right-hand sides."""
     import numpy as np
@@ -623,15 +623,16 @@ def kernel_only(name, reps, iters=24, ordering="natural", nsys=64):
         torch.cuda.synchronize()
         print(json.dumps({"kernel_only": name, "n": n, "p": P_RHS, "reps": reps, "loss": loss}))
         return
-    J = bpf.grid.preset_jacobian("case70k", 0)
+    J = bpf.grid.preset_jacobian(kgrid, 0)
     n = J.shape[0]
-    p = 128
+    p = kp
     A = bpf.CuSparseMatrixCSR.from_scipy(J)
     X = bpf.colmajor(torch.randn(n, p, dtype=torch.float64, device="cuda"))
     Y = bpf.empty_colmajor(n, p)
     if name in ("trsv", "factor"):
-        P = bpf.ilu0(A, p)
-    for _ in range(reps):
+        P = bpf.ilu0(A, p, ordering=ordering)
+
+    def run():
         if name == "trsv":
             bpf.ldiv_(Y, P, X)
         elif name == "spmm":
@@ -639,9 +640,29 @@ def kernel_only(name, reps, iters=24, ordering="natural", nsys=64):
         elif name == "factor":
             P.refactor(A.nzVal)
         elif name == "gram":
-            bpf.householder(X[:, :64])
+            bpf.householder(X[:, :64], lapack=False)
+
+    out = {"kernel_only": name, "grid": kgrid, "n": n, "p": p, "ordering": ordering, "reps": reps}
+    if timed:
+        # 3 warm-up launches, then `reps` launches timed by the library's per-class CUDA events
+        for _ in range(3):
+            run()
+        bpf._lib.set_timing(True)
+        for _ in range(reps):
+            run()
+        torch.cuda.synchronize()
+        out["timing"] = _class_rates(bpf, (name,))
+        bpf._lib.set_timing(False)
+        hbm, src = peaks()
+        for v in out["timing"].values():
+            if v.get("GBps"):
+                v["frac_of_hbm"] = v["GBps"] / hbm
+                v["peak_source"] = src
+    else:
+        for _ in range(reps):
+            run()
     torch.cuda.synchronize()
-    print(json.dumps({"kernel_only": name, "n": n, "p": p, "reps": reps}))
+    print(json.dumps(out))
 
 
 def _class_rates(bpf, classes):
@@ -1166,6 +1187,9 @@ def main():
     ap.add_argument("--iters", type=int, default=24, help="block-GMRES iterations (--kernel-only gmres)")
     ap.add_argument("--ordering", default="natural", help="ILU(0) ordering (--kernel-only gmres)")
     ap.add_argument("--nsys", type=int, default=64, help="systems of the batch (--kernel-only batch)")
+    ap.add_argument("--grid", default="case70k", help="preset grid of --kernel-only trsv/spmm/factor/gram")
+    ap.add_argument("--p", type=int, default=128, help="right-hand sides of --kernel-only trsv/spmm")
+    ap.add_argument("--time", action="store_true", help="--kernel-only: time the launches (CUDA events)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -1177,7 +1201,8 @@ def main():
                          "each for the other benchmark configurations")
     args = ap.parse_args()
     if args.kernel_only:
-        kernel_only(args.kernel_only, args.reps, args.iters, args.ordering, args.nsys)
+        kernel_only(args.kernel_only, args.reps, args.iters, args.ordering, args.nsys, args.grid, args.p,
+                    args.time)
         return
     if args.config in ("gmres300", "bicgstab9k", "rf25k", "newton9k"):
         {"gmres300": config_gmres300, "bicgstab9k": config_bicgstab9k,

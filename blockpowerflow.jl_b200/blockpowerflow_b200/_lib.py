@@ -90,6 +90,7 @@ SIGNATURES = {
                                  C.POINTER(_D), C.POINTER(_D)]),
     "bpf_spmm": (_I, [_P, C.POINTER(CsrDesc), _I, _D, _P, _I, _D, _P, _I]),
     "bpf_householder": (_I, [_P, _I, _I, _P, _I, _P, _I]),
+    "bpf_householder_lapack": (_I, [_P, _I, _I, _P, _I, _P, _I, _P, _I]),
     "bpf_ilu0_create": (_I, [_P, C.POINTER(CsrDesc), _I, _I, C.POINTER(_P)]),
     "bpf_ic0_create": (_I, [_P, C.POINTER(CsrDesc), _I, _I, C.POINTER(_P)]),
     "bpf_ilu0_create_ordered": (_I, [_P, C.POINTER(CsrDesc), _I, _I, _I, C.POINTER(_P)]),

@@ -110,9 +110,13 @@ def mul(A: CuSparseMatrixCSR, X, alpha: float = 1.0, beta: float = 0.0, Y=None):
     return Y
 
 
-def householder(A):
-    """householder(A) on an n x p device block: returns (Q, R) with Q^T Q = I, Q R = A
-    (src/block_utils.jl:38-53).  A is not modified."""
+def householder(A, compact: bool = False, lapack: bool = True):
+    """householder(A; compact) on an n x p device block (src/block_utils.jl:38-53): returns
+    (Q, R) with LAPACK's conventions -- Q^T Q = I and Q R = A (orgqr's Q), or with compact=True
+    geqrf's compact form in Q (R above, the reflector vectors below the diagonal); the
+    reflectors' tau are kept as the attribute `householder.tau` of the last call.  lapack=False
+    returns the Cholesky-QR2 factors themselves (R with a positive diagonal).  A is not
+    modified."""
     import torch
 
     Qc = colmajor(A)
@@ -122,5 +126,13 @@ def householder(A):
     R = torch.zeros((p, p), dtype=torch.float64, device=Qc.device).t()
     lib = _lib.load()
     ctx = _lib.context(Qc.device.index)
-    _lib.check(lib.bpf_householder(ctx, n, p, Qc.data_ptr(), ld(Qc), R.data_ptr(), p), ctx)
+    if not lapack:
+        if compact:
+            raise ValueError("compact=True needs the LAPACK form (lapack=True)")
+        _lib.check(lib.bpf_householder(ctx, n, p, Qc.data_ptr(), ld(Qc), R.data_ptr(), p), ctx)
+        return Qc, R
+    tau = torch.zeros(p, dtype=torch.float64, device=Qc.device)
+    _lib.check(lib.bpf_householder_lapack(ctx, n, p, Qc.data_ptr(), ld(Qc), R.data_ptr(), p, tau.data_ptr(),
+                                          int(bool(compact))), ctx)
+    householder.tau = tau
     return Qc, R

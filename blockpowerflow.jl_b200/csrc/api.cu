@@ -176,6 +176,10 @@ bpf_status prec_setup(bpf_ctx *ctx, int kind, int n, const std::vector<int> &rp,
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(*d, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, ctx->stream);
     };
+    if (kind != PREC_LU && n > 0) {
+        if (e == cudaSuccess) e = cudaMalloc((void **)&P->sf_flags, sizeof(unsigned) * n);
+        if (e == cudaSuccess) e = cudaMemsetAsync(P->sf_flags, 0, sizeof(unsigned) * n, ctx->stream);
+    }
     up_i(&P->rp, rp);
     up_i(&P->ci, ci);
     up_i(&P->diag, diag);
@@ -609,6 +613,7 @@ bpf_status bpf_prec_destroy(bpf_prec *P) {
     cudaFree(P->perm);
     cudaFree(P->amap);
     cudaFree(P->zbuf);
+    cudaFree(P->sf_flags);
     cudaFree(P->cl_lev_ptr);
     cudaFree(P->cl_ent);
     cudaFree(P->bj_rows);

@@ -948,6 +948,120 @@ bpf_status frob_norm(bpf_ctx *ctx, size_t len, const double *x, double *out) {
 // ---------------------------------------------------------------------------------------
 using namespace bpf;
 
+namespace bpf {
+
+// Householder vectors of an orthonormal Q (row-major n x p, positive-diagonal R from Cholesky-QR)
+// in LAPACK's geqrf form, by reconstruction (Ballard et al., "Reconstructing Householder vectors
+// from tall-skinny QR", 2015): the LU without pivoting of Q - [S; 0], where the sign s_j is taken
+// opposite to the running pivot, gives the unit lower trapezoidal Y = [Y1; Y2] of the reflectors
+// and U = -T Y1^T S, so tau_j = T_jj = -U_jj s_j; Q S is what orgqr returns and S R its R (the
+// R of Householder QR applied to the original block, with LAPACK's signs).  One CTA: the p x p
+// top block is factored in shared memory (s_j, tau_j, strict lower L1 = Y1), U^{-1} is formed by
+// column-wise back substitution (a thread per column) for Y2 = Q2 U^{-1}.
+__global__ void house_recon_kernel(int p, const double *__restrict__ Qtop, const double *__restrict__ R,
+                                   double *__restrict__ sgn, double *__restrict__ tau,
+                                   double *__restrict__ Uinv, double *__restrict__ Ctop) {
+    extern __shared__ double M[];   // p x p, row-major
+    __shared__ double s_piv;
+    for (int idx = threadIdx.x; idx < p * p; idx += blockDim.x) M[idx] = Qtop[idx];
+    __syncthreads();
+    for (int j = 0; j < p; j++) {
+        if (threadIdx.x == 0) {
+            const double a = M[j * p + j];
+            const double s = a >= 0.0 ? -1.0 : 1.0;   // LAPACK: beta = -sign(alpha) ||x||
+            sgn[j] = s;
+            M[j * p + j] = a - s;                      // |a - s| >= 1
+            s_piv = a - s;
+        }
+        __syncthreads();
+        const double piv = s_piv;
+        for (int i = j + 1 + threadIdx.x; i < p; i += blockDim.x) M[i * p + j] /= piv;
+        __syncthreads();
+        const int rows = p - j - 1;
+        for (int idx = threadIdx.x; idx < rows * rows; idx += blockDim.x) {
+            const int i = j + 1 + idx / rows, k = j + 1 + idx % rows;
+            M[i * p + k] -= M[i * p + j] * M[j * p + k];
+        }
+        __syncthreads();
+    }
+    // tau, the compact top block (upper: S R; strict lower: L1) and U^{-1}
+    for (int idx = threadIdx.x; idx < p * p; idx += blockDim.x) {
+        const int i = idx / p, k = idx % p;
+        Ctop[idx] = k >= i ? sgn[i] * R[idx] : M[idx];
+    }
+    for (int j = threadIdx.x; j < p; j += blockDim.x) tau[j] = -M[j * p + j] * sgn[j];
+    for (int k = threadIdx.x; k < p; k += blockDim.x) {
+        for (int i = p - 1; i >= 0; i--) {
+            if (i > k) {
+                Uinv[i * p + k] = 0.0;
+                continue;
+            }
+            double v = (i == k) ? 1.0 : 0.0;
+            for (int l = i + 1; l <= k; l++) v -= M[i * p + l] * Uinv[l * p + k];
+            Uinv[i * p + k] = v / M[i * p + i];
+        }
+    }
+}
+
+// Columns of a row-major n x p block scaled by s (Q S), rows of a p x p matrix (S R).
+__global__ void scale_cols_kernel(size_t n, int p, const double *__restrict__ s, double *__restrict__ X) {
+    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n * p; idx += (size_t)gridDim.x * blockDim.x)
+        X[idx] *= s[idx % p];
+}
+__global__ void scale_rows_kernel(int p, const double *__restrict__ s, double *__restrict__ R) {
+    for (int idx = threadIdx.x; idx < p * p; idx += blockDim.x) R[idx] *= s[idx / p];
+}
+
+}  // namespace bpf
+
+extern "C" bpf_status bpf_householder_lapack(bpf_ctx *ctx, int n, int p, double *Q, int ldq, double *R,
+                                             int ldr, double *tau, int compact) {
+    if (!ctx) return BPF_ERR_INVALID_VALUE;
+    if (n < 0 || p < 0 || (n > 0 && p > 0 && (!Q || !R)))
+        return set_error(ctx, BPF_ERR_INVALID_VALUE, "householder: invalid argument");
+    if (ldq < std::max(1, n) || ldr < std::max(1, p))
+        return set_error(ctx, BPF_ERR_DIMENSION, "householder: leading dimension too small");
+    if (p > n) return set_error(ctx, BPF_ERR_DIMENSION, "householder: n=%d < p=%d", n, p);
+    if (n == 0 || p == 0) return BPF_SUCCESS;
+    if (p > 128) return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "householder: p=%d > 128", p);
+    const size_t np = (size_t)n * p, pp = (size_t)p * p;
+    bpf_status s;
+    double *buf = (double *)ws_get(ctx, WS_A, sizeof(double) * (3 * np + 4 * pp + 2 * (size_t)p), &s);
+    if (!buf) return s;
+    double *W = buf, *Qr = buf + np, *T = buf + 2 * np, *Rr = buf + 3 * np, *Uinv = Rr + pp, *Ctop = Uinv + pp,
+           *Rl = Ctop + pp, *sg = Rl + pp, *tau_d = sg + p;
+    SolveState *st = (SolveState *)ws_get(ctx, WS_STATE, sizeof(SolveState), &s);
+    if (!st) return s;
+    SolveState hs;
+    memset(&hs, 0, sizeof(hs));
+    hs.active = 1;
+    BPF_CUDA(ctx, cudaMemcpyAsync(st, &hs, sizeof(SolveState), cudaMemcpyHostToDevice, ctx->stream));
+    BPF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    BPF_TRY(colmajor_to_rowmajor(ctx, n, p, Q, ldq, W));
+    BPF_TRY(cholqr(ctx, n, p, W, Qr, Rr, T, st));
+    const size_t smem = sizeof(double) * pp;
+    BPF_CUDA(ctx, cudaFuncSetAttribute(house_recon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    house_recon_kernel<<<1, 256, smem, ctx->stream>>>(p, Qr, Rr, sg, tau_d, Uinv, Ctop);
+    BPF_LAUNCHED(ctx);
+    BPF_CUDA(ctx, cudaMemcpyAsync(Rl, Rr, sizeof(double) * pp, cudaMemcpyDeviceToDevice, ctx->stream));
+    scale_rows_kernel<<<1, 256, 0, ctx->stream>>>(p, sg, Rl);
+    BPF_LAUNCHED(ctx);
+    if (compact) {
+        // [Ctop; Q2 U^{-1}] in W (row-major), then to the caller's column-major Q
+        BPF_CUDA(ctx, cudaMemcpyAsync(W, Ctop, sizeof(double) * pp, cudaMemcpyDeviceToDevice, ctx->stream));
+        if (n > p) BPF_TRY(tsmm(ctx, n - p, p, 1, Qr + pp, 0, Uinv, 0, 1.0, nullptr, 0.0, W + pp, st));
+        BPF_TRY(rowmajor_to_colmajor(ctx, n, p, W, Q, ldq));
+    } else {
+        const int g = (int)std::max<long long>(1, std::min<long long>(ceil_div((long long)np, 256LL), 4LL * ctx->num_sms));
+        scale_cols_kernel<<<g, 256, 0, ctx->stream>>>(n, p, sg, Qr);
+        BPF_LAUNCHED(ctx);
+        BPF_TRY(rowmajor_to_colmajor(ctx, n, p, Qr, Q, ldq));
+    }
+    BPF_TRY(rowmajor_to_colmajor(ctx, p, p, Rl, R, ldr));
+    if (tau) BPF_CUDA(ctx, cudaMemcpyAsync(tau, tau_d, sizeof(double) * p, cudaMemcpyDeviceToDevice, ctx->stream));
+    return check_dev_status(ctx, "householder");
+}
+
 extern "C" bpf_status bpf_householder(bpf_ctx *ctx, int n, int p, double *Q, int ldq, double *R,
                                       int ldr) {
     if (!ctx) return BPF_ERR_INVALID_VALUE;

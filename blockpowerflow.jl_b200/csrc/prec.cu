@@ -25,6 +25,8 @@
 #include <system_error>
 #include <thread>
 
+#include <cstdlib>
+
 #include "bpf_internal.cuh"
 #include "prec.cuh"
 
@@ -665,10 +667,167 @@ static bpf_status launch_trsv2(bpf_ctx *ctx, const TriDev &t0, const TriDev &t1,
     return BPF_SUCCESS;
 }
 
+// ------------------------------------------------------------------------------------
+// Sync-free triangular solves (p >= 17: a warp per row, lanes over the right-hand sides).
+//
+// The level-scheduled kernel above separates every dependency level by a grid barrier (~5 us
+// each, 26 + 26 of them on the 9,000-bus minimum-degree factors).  Here the rows of a sweep are
+// taken in level order, position q by warp q mod W (W = all warps of the co-resident grid), and
+// a row waits only for the rows it reads: lane l polls the ready word of the row of entry l
+// (acquire), the warp proceeds when all its lanes have seen theirs.  A producer writes its row,
+// then publishes it (fence + release store of the word).  No deadlock: the pending row of
+// smallest position has all its inputs done (they sit at smaller positions), and its warp is
+// resident (cooperative launch) and has finished its earlier positions, so it runs.  Every poll
+// is bounded by the context's wait limit; a warp that gives up records the timeout and returns,
+// so the rows waiting on it give up too.  One grid barrier separates the two sweeps (the
+// backward sweep overwrites in place what forward rows may still read when the pattern is not
+// symmetric).  Ready words: 2e after the forward sweep of launch e, 2e + 1 after the backward
+// sweep, so they are monotone and never reset.  Same arithmetic, summation order and
+// permutation handling as trsv2_coop_kernel, so the results are bit-identical.
+// ------------------------------------------------------------------------------------
+template <int CPL, typename TF>
+__global__ void __launch_bounds__(512)
+trsv_sf_kernel(TriKernelArgs t0, TriKernelArgs t1, int p, const double *X, double *Yout,
+               DevStatus *ds, const int *gate, const int *perm, double *Zv, unsigned *flags,
+               unsigned epoch) {
+    __shared__ unsigned s_gen;
+    __shared__ int s_skip;
+    if (threadIdx.x == 0) s_gen = barrier_gen_start(ds);
+    __syncthreads();
+    unsigned gen = s_gen;
+    if (gate) {   // one decision for the grid, as in trsv2_coop_kernel
+        if (blockIdx.x == 0 && threadIdx.x == 0) ds->pad[0] = (*gate == 0) ? 1 : 0;
+        if (!grid_barrier(ds, gen)) return;
+        if (threadIdx.x == 0) s_skip = ld_relaxed_i32(&ds->pad[0]);
+        __syncthreads();
+        if (s_skip) return;
+    }
+    double *Zf = perm ? Zv : Yout;
+    const int lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    const long long lim = ds->wait_limit > 0 ? ds->wait_limit : kSpinLimit;
+    bool alive = true;
+#pragma unroll 1
+    for (int phase = 0; phase < 2; phase++) {
+        const TriKernelArgs &t = phase == 0 ? t0 : t1;
+        const TF *val = std::is_same<TF, float>::value ? (const TF *)t.valf : (const TF *)t.val;
+        const TF *dinv = std::is_same<TF, float>::value ? (const TF *)t.dinvf : (const TF *)t.dinv;
+        const unsigned want = 2u * epoch + (unsigned)phase;   // ready word of a row this sweep reads
+        double *Y = phase == 0 ? Zf : Yout;                     // the sweep's solved rows
+        for (int q = wid; alive && q < t.n; q += nw) {
+            const int i = __ldg(t.rows + q);
+            const int io = perm ? __ldg(perm + i) : i;   // row of i in the caller's order
+            TF acc[CPL];
+#pragma unroll
+            for (int j = 0; j < CPL; j++) {
+                const int col = lane + j * 32;
+                if (col < p) {
+                    if (phase == 0) acc[j] = (TF)X[(size_t)io * p + col];
+                    else acc[j] = (TF)__ldcg(Zf + (size_t)i * p + col);
+                } else {
+                    acc[j] = (TF)0;
+                }
+            }
+            const int rs = __ldg(t.rp + q), re = __ldg(t.rp + q + 1);
+            for (int kb = rs; kb < re; kb += 32) {
+                const int k = kb + lane;
+                int c = 0;
+                TF a = (TF)0;
+                bool ok = true;
+                if (k < re) {
+                    c = __ldg(t.ci + k);
+                    a = __ldg(val + k);
+                    // bounded wait for row c of this sweep
+                    long long it = 0;
+                    while (ld_acquire_u32(flags + c) < want) {
+                        if (++it > lim || ld_relaxed_i32(&ds->err) != 0) {
+                            ok = false;
+                            break;
+                        }
+                        __nanosleep(32);
+                    }
+                }
+                __syncwarp();   // orders every lane's acquire before the warp's reads of those rows
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (!ok) atomicCAS(&ds->err, 0, (int)DEV_BARRIER_TIMEOUT);
+                    alive = false;
+                    break;
+                }
+                const int cnt = min(32, re - kb);
+                int co = 0;
+                if (k < re && perm && phase == 1) co = __ldg(perm + c);
+#pragma unroll 4   // several entries' loads in flight; same summation order as the level kernel
+                for (int s = 0; s < cnt; s++) {
+                    const int cs = __shfl_sync(0xffffffffu, (perm && phase == 1) ? co : c, s);
+                    const TF as = __shfl_sync(0xffffffffu, a, s);
+                    const double *yr = Y + (size_t)cs * p;
+#pragma unroll
+                    for (int j = 0; j < CPL; j++) {
+                        const int col = lane + j * 32;
+                        if (col < p) acc[j] -= as * (TF)__ldcg(yr + col);
+                    }
+                }
+            }
+            if (!alive) break;
+            TF dv = (TF)1;
+            if (dinv) dv = __ldg(dinv + q);
+            double *yi = Y + (size_t)((phase == 1) ? io : i) * p;
+#pragma unroll
+            for (int j = 0; j < CPL; j++) {
+                const int col = lane + j * 32;
+                if (col < p) yi[col] = (double)(acc[j] * dv);
+            }
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence();
+                st_release_u32(flags + i, 2u * epoch + (unsigned)phase);
+            }
+        }
+        if (phase == 0) {
+            // every CTA reaches this barrier: a warp that gave up still arrives (its CTA's
+            // threads all call it), and the barrier itself sees the pending error
+            if (!grid_barrier(ds, gen)) return;
+            if (!alive) return;
+        }
+    }
+}
+
+template <int CPL, typename TF>
+static bpf_status launch_trsv_sf(bpf_ctx *ctx, const TriDev &t0, const TriDev &t1, int p, const void *X,
+                                 void *Y, const int *gate, const int *perm, double *Z, unsigned *flags,
+                                 unsigned epoch) {
+    auto kern = trsv_sf_kernel<CPL, TF>;
+    int per_sm = 0;
+    BPF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 512, 0));
+    if (per_sm < 1) return set_error(ctx, BPF_ERR_CUDA, "sync-free triangular solve does not fit on an SM");
+    // every warp resident; no more warps than rows of the larger sweep
+    const int grid = std::max(1, std::min(per_sm * ctx->num_sms, ceil_div(std::max(t0.n, 1), 16)));
+    TriKernelArgs a0 = t0.args(), a1 = t1.args();
+    DevStatus *ds = ctx->dstat;
+    void *args[] = {&a0, &a1, &p, (void *)&X, &Y, &ds, (void *)&gate, (void *)&perm, &Z, &flags, &epoch};
+    const double fb = (4.0 + sizeof(TF)) * ((double)t0.nnz + t1.nnz) + sizeof(TF) * (double)t0.n +
+                      16.0 * (t0.n + 1) + 8.0 * t0.n;
+    const double vb = (double)t0.n * p * 32.0;
+    KScope ks(ctx, BPF_KC_TRSV, fb + vb, 2.0 * ((double)t0.nnz + t1.nnz + t0.n) * p);
+    BPF_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)kern, dim3(grid), dim3(512), args, 0, ctx->stream));
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
 template <typename TF, bool IN_F32, bool OUT_F32>
 static bpf_status trsv2_dispatch(bpf_ctx *ctx, const TriDev &t0, const TriDev &t1, int p,
                                  const void *X, void *Y, const int *gate, const int *perm,
-                                 double *Z) {
+                                 double *Z, unsigned *flags = nullptr, unsigned epoch = 0) {
+    // sync-free for blocks of 17..256 columns whose level-scheduled launch would span several CTAs
+    static const bool levels_only = getenv("BPF_TRSV_LEVELS") && atoi(getenv("BPF_TRSV_LEVELS")) != 0;
+    if (!IN_F32 && !OUT_F32 && flags && !levels_only && p > 16 && p <= 256 &&
+        std::max(t0.max_level_rows, t1.max_level_rows) > 2 * (512 / 32)) {
+        if (p <= 32) return launch_trsv_sf<1, TF>(ctx, t0, t1, p, X, Y, gate, perm, Z, flags, epoch);
+        if (p <= 64) return launch_trsv_sf<2, TF>(ctx, t0, t1, p, X, Y, gate, perm, Z, flags, epoch);
+        if (p <= 128) return launch_trsv_sf<4, TF>(ctx, t0, t1, p, X, Y, gate, perm, Z, flags, epoch);
+        return launch_trsv_sf<8, TF>(ctx, t0, t1, p, X, Y, gate, perm, Z, flags, epoch);
+    }
     if (p <= 4) return launch_trsv2<4, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate, perm, Z);
     if (p <= 8) return launch_trsv2<8, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate, perm, Z);
     if (p <= 16) return launch_trsv2<16, 1, TF, IN_F32, OUT_F32>(ctx, t0, t1, p, X, Y, gate, perm, Z);
@@ -690,8 +849,10 @@ bpf_status prec_apply_rowmajor(bpf_ctx *ctx, const bpf_prec *P, int p, const dou
                          "reordered preconditioner: %d right-hand sides exceed the %d-column scratch "
                          "reserved for it", p, P->zcols);
     if (P->fdtype == BPF_F32)
-        return trsv2_dispatch<float, false, false>(ctx, P->lower, P->upper, p, X, Y, gate, P->perm, P->zbuf);
-    return trsv2_dispatch<double, false, false>(ctx, P->lower, P->upper, p, X, Y, gate, P->perm, P->zbuf);
+        return trsv2_dispatch<float, false, false>(ctx, P->lower, P->upper, p, X, Y, gate, P->perm, P->zbuf,
+                                                   P->sf_flags, ++P->sf_epoch);
+    return trsv2_dispatch<double, false, false>(ctx, P->lower, P->upper, p, X, Y, gate, P->perm, P->zbuf,
+                                                P->sf_flags, ++P->sf_epoch);
 }
 
 bpf_status prec_reserve_z(bpf_ctx *ctx, bpf_prec *P, int p) {

