@@ -125,6 +125,7 @@ SIGNATURES = {
     "bpf_rf_refactor": (_I, [_P, _P]),
     "bpf_rf_refactor_batch": (_I, [_P, _P, _I]),
     "bpf_rf_solve": (_I, [_P, _I, _P, _I]),
+    "bpf_rf_solve_refined": (_I, [_P, C.POINTER(CsrDesc), _I, _P, _I, _P, _I, _I]),
     "bpf_rf_info": (_I, [_P, C.POINTER(_I), C.POINTER(_I), _P, _P]),
     "bpf_rf_destroy": (_I, [_P]),
     "bpf_batch_opts_default": (None, [C.POINTER(BatchOpts)]),

@@ -19,7 +19,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from .sparse import CuSparseMatrixCSR, colmajor, ld
+from .sparse import CuSparseMatrixCSR, colmajor, empty_colmajor, ld
 
 
 class _RfBase:
@@ -60,6 +60,18 @@ class _RfBase:
             raise ValueError("X must be a column-major block")
         n, p = X.shape
         _lib.check(_lib.load().bpf_rf_solve(self._h, p, X.data_ptr(), ld(X)), self._ctx)
+
+    def solve_refined(self, A: CuSparseMatrixCSR, B, steps: int = 1):
+        """X = A \\ B with `steps` rounds of iterative refinement on the refactored LU (A: the
+        matrix of the last update!, with its current values).  An addition: the reference's
+        ldiv! applies the LU once."""
+        Bc = colmajor(B)
+        n, p = Bc.shape
+        X = empty_colmajor(n, p, Bc.device)
+        d = A.desc()
+        _lib.check(_lib.load().bpf_rf_solve_refined(self._h, C.byref(d), p, Bc.data_ptr(), ld(Bc), X.data_ptr(),
+                                                    ld(X), int(steps)), self._ctx)
+        return X
 
     def destroy(self):
         h = getattr(self, "_h", None)

@@ -138,6 +138,15 @@ static int sparse_lu(int n, const std::vector<int> &cp, const std::vector<int> &
 // device helpers: permuted layout conversions and value scatter
 // ------------------------------------------------------------------------------------
 // dst[i][c] = src[c*ld + perm[i]]  (column-major -> row-major, gathering rows)
+// X (column-major, ld ldx) += R (n x p, ld n).
+__global__ void cm_add_kernel(int n, int p, const double *__restrict__ R, double *__restrict__ X, int ldx) {
+    const size_t len = (size_t)n * p;
+    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < len; idx += (size_t)gridDim.x * blockDim.x) {
+        const size_t c = idx / n, r = idx - c * n;
+        X[c * ldx + r] += R[idx];
+    }
+}
+
 __global__ void cm_to_rm_perm_kernel(int n, int p, const double *__restrict__ src, int ld,
                                      const int *__restrict__ perm, double *__restrict__ dst) {
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < (size_t)n * p;
@@ -415,6 +424,43 @@ bpf_status bpf_rf_solve(bpf_rf *rf, int nrhs, double *X, int ldx) {
         P->upper.val = uv0;
         P->upper.dinv = dv0;
         if (st != BPF_SUCCESS) return st;
+    }
+    return BPF_SUCCESS;
+}
+
+bpf_status bpf_rf_solve_refined(bpf_rf *rf, const bpf_csr_desc *A, int nrhs, const double *B, int ldb,
+                                double *X, int ldx, int steps) {
+    if (!rf) return BPF_ERR_INVALID_VALUE;
+    bpf_ctx *ctx = rf->ctx;
+    const int n = rf->n;
+    if (!A || nrhs < 0 || steps < 0 || (nrhs > 0 && n > 0 && (!B || !X)))
+        return set_error(ctx, BPF_ERR_INVALID_VALUE, "rf_solve_refined: invalid argument");
+    if (A->n != n || A->nnz != rf->nnzA)
+        return set_error(ctx, BPF_ERR_DIMENSION, "rf_solve_refined: A is not the analysed matrix");
+    if (ldb < std::max(1, n) || ldx < std::max(1, n))
+        return set_error(ctx, BPF_ERR_DIMENSION, "rf_solve_refined: leading dimension < n");
+    if (!rf->uniform)
+        return set_error(ctx, BPF_ERR_NOT_SUPPORTED, "rf_solve_refined: replicas with distinct values");
+    if (rf->batch > 1 && nrhs != rf->batch)
+        return set_error(ctx, BPF_ERR_DIMENSION, "batch mode solves exactly batchsize=%d columns", rf->batch);
+    if (n == 0 || nrhs == 0) return BPF_SUCCESS;
+    BPF_CUDA(ctx, cudaMemcpy2DAsync(X, sizeof(double) * ldx, B, sizeof(double) * ldb, sizeof(double) * n, nrhs,
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
+    BPF_TRY(bpf_rf_solve(rf, nrhs, X, ldx));
+    if (steps == 0) return BPF_SUCCESS;
+    bpf_status st;
+    double *R = (double *)ws_get(ctx, WS_C, sizeof(double) * (size_t)n * nrhs, &st);
+    if (!R) return st;
+    for (int k = 0; k < steps; k++) {
+        // R = B - A X, then X += LU \ R
+        BPF_CUDA(ctx, cudaMemcpy2DAsync(R, sizeof(double) * n, B, sizeof(double) * ldb, sizeof(double) * n, nrhs,
+                                        cudaMemcpyDeviceToDevice, ctx->stream));
+        BPF_TRY(bpf_spmm(ctx, A, nrhs, -1.0, X, ldx, 1.0, R, n));
+        BPF_TRY(bpf_rf_solve(rf, nrhs, R, n));
+        const size_t len = (size_t)n * nrhs;
+        const int blocks = std::max(1, std::min(ceil_div((long long)len, 256), ctx->num_sms * 8));
+        cm_add_kernel<<<blocks, 256, 0, ctx->stream>>>(n, nrhs, R, X, ldx);
+        BPF_LAUNCHED(ctx);
     }
     return BPF_SUCCESS;
 }

@@ -422,6 +422,14 @@ BPF_API bpf_status bpf_rf_refactor_batch(bpf_rf *rf, const double *vals, int ld)
  * (multi-RHS; the reference allows only nrhs = 1, :228-230).  Batch mode requires
  * nrhs == batch and solves column r with replica r. */
 BPF_API bpf_status bpf_rf_solve(bpf_rf *rf, int nrhs, double *X, int ldx);
+/* X = A \ B by the refactored LU followed by `steps` rounds of iterative refinement
+ * (X += LU \ (B - A X), residual in FP64 with A's current values: the matrix given to the last
+ * bpf_rf_refactor, as a device CSR descriptor).  No counterpart in the reference, whose
+ * cusolverRf solve (src/cusolverRF.jl:317-331) applies the refactored LU once; a refactorization
+ * that keeps the analysis's pivot order on new values can lose a digit or two to growth, and one
+ * round recovers them.  B and X are distinct column-major blocks; uniform factors only. */
+BPF_API bpf_status bpf_rf_solve_refined(bpf_rf *rf, const bpf_csr_desc *A, int nrhs, const double *B,
+                                        int ldb, double *X, int ldx, int steps);
 /* nnz of L (strict lower) and U (incl. diagonal), and the host-side P/Q permutations
  * (0-based, n ints each; nullable). */
 BPF_API bpf_status bpf_rf_info(const bpf_rf *rf, int *nnzL, int *nnzU, int *P, int *Q);
