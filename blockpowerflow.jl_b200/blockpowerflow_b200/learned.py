@@ -148,30 +148,108 @@ def train(mlp: WarmStartMLP, pairs, *, epochs: int = 10, lr: float = 2e-4, batch
     return hist
 
 
-def judged_warm_start(mlp: WarmStartMLP, A: CuSparseMatrixCSR, B):
-    """The network's warm start if its residual ||B - A X0||_F is below ||B||_F (the zero
-    start's), else None: plain block-GMRES judges the network and falls back to it."""
+def judged_warm_start(mlp: WarmStartMLP, A: CuSparseMatrixCSR, B, N=None):
+    """The network's warm start if it beats the zero start, else None: plain block-GMRES judges
+    the network and falls back to it.  Without a preconditioner the test is the residual,
+    ||B - A X0||_F < ||B||_F.  With the right preconditioner N (an approximate inverse of A) it is
+    the estimated error, ||N \\ (B - A X0)||_F < ||N \\ B||_F: the network's misses are mostly
+    short-wavelength components that A amplifies in the residual while the preconditioner removes
+    them in the first iteration, so the residual alone would discard useful starts."""
     import torch
 
+    from .precond import ldiv_
     from .sparse import mul
 
     Bc = colmajor(B)
     X0 = mlp.forward(Bc)
     R = Bc.clone()   # a copy with Bc's (column-major) strides; B itself is left untouched
     mul(A, X0, alpha=-1.0, beta=1.0, Y=R)
-    return X0 if float(torch.linalg.norm(R)) < float(torch.linalg.norm(Bc)) else None
+    if N is None:
+        return X0 if float(torch.linalg.norm(R)) < float(torch.linalg.norm(Bc)) else None
+    E = empty_colmajor(Bc.shape[0], Bc.shape[1], Bc.device)
+    ldiv_(E, N, R)
+    e0 = float(torch.linalg.norm(E))
+    ldiv_(E, N, Bc)
+    return X0 if e0 < float(torch.linalg.norm(E)) else None
 
 
 def solve(A: CuSparseMatrixCSR, B, N, mlp: WarmStartMLP, Z=None, *, rtol: float = 1e-8,
-          itmax: int = 300):
+          itmax: int = 300, judge: str = "error"):
     """Right-preconditioned block-GMRES from the judged warm start, augmented with the learned
-    deflation basis Z (if given); the tolerance is rtol ||B||_F whatever the start."""
+    deflation basis Z (if given); the tolerance is rtol ||B||_F whatever the start.  judge:
+    "error" (the preconditioned residual, the default) or "residual" (judged_warm_start)."""
     import torch
 
     from .krylov import block_gmres
 
     Bc = colmajor(B)
-    X0 = judged_warm_start(mlp, A, Bc)
+    X0 = judged_warm_start(mlp, A, Bc, N if judge == "error" else None)
     nb = float(torch.linalg.norm(Bc))
     return block_gmres(A, Bc, X0, N=N, ldiv=True, restart=False, memory=itmax, atol=rtol * nb,
                        rtol=0.0, itmax=itmax, deflation=Z)
+
+
+# ---- the sensitivity family: solves the Newton caller makes along a sequence of operating points
+class SensitivityFamily:
+    """Right-hand sides of the Newton caller's sensitivity solves (benchmarks_nvidia.jl:29-39
+    solves Gx X = Gu) along a sequence of nearby operating points of one grid.
+
+    Point t: the state x_t = the solution's, perturbed by N(0, sigma) in every angle and PQ
+    magnitude (newton.perturbed_start with seed `seed + t`); Gx(x_t) is assembled on the device
+    into A's values, Gu(x_t) into a device block, and the block's right-hand sides are the
+    columns of Gu(x_t) for p controls drawn (seeded by t) from a fixed set of controls of interest
+    (`controls`, default: up to 512 of the grid's slack / PV controls)."""
+
+    def __init__(self, prob, A: CuSparseMatrixCSR, p: int, *, controls=None, sigma: float = 0.001,
+                 seed: int = 0):
+        import torch
+
+        from . import newton as NT
+
+        self.prob, self.A, self.p, self.sigma, self.seed = prob, A, int(p), float(sigma), int(seed)
+        self.asm = NT.DeviceAssembly(prob, A)
+        nc = self.asm.n_ctrl
+        if controls is None:
+            rng = np.random.default_rng(seed)
+            controls = np.sort(rng.choice(nc, size=min(512, nc), replace=False))
+        self.controls = np.asarray(controls, dtype=np.int64)
+        if self.p > len(self.controls):
+            raise ValueError(f"p = {p} exceeds the {len(self.controls)} controls of interest")
+        dev = A.nzVal.device
+        self.Gu = torch.empty((nc, self.asm.n), dtype=torch.float64, device=dev).t()   # column-major
+        self._dev = dev
+
+    def point(self, t: int):
+        """Assemble point t: A's values become Gx(x_t); returns B_t (column-major n x p)."""
+        import torch
+
+        from . import newton as NT
+
+        x = NT.perturbed_start(self.prob, self.sigma, seed=self.seed + t)
+        self.asm.jacobian(torch.as_tensor(x, device=self._dev), self.Gu)
+        rng = np.random.default_rng(1_000_003 + 7919 * self.seed + t)
+        cols = np.sort(rng.choice(self.controls, size=self.p, replace=False))
+        idx = torch.as_tensor(cols, device=self._dev)
+        return colmajor(self.Gu.index_select(1, idx))
+
+
+def family_pairs(fam: SensitivityFamily, N, points, *, rtol: float = 1e-10, itmax: int = 400):
+    """Training data the solver generates on the family: for each point t, B_t and its plain
+    ILU(0) block-GMRES solution (N refactored at the point).  Returns [(B_t, X_t)] (device,
+    column-major) and the median ||x|| / ||b||."""
+    import torch
+
+    from .krylov import block_gmres
+
+    pairs, ratios = [], []
+    for t in points:
+        B = fam.point(t)
+        N.refactor(fam.A.nzVal)
+        X, st = block_gmres(fam.A, B, N=N, ldiv=True, restart=False, memory=itmax, atol=0.0, rtol=rtol,
+                            itmax=itmax)
+        if not st.solved:
+            continue
+        pairs.append((B, X))
+        ratios.append((torch.linalg.norm(X, dim=0) / torch.linalg.norm(B, dim=0)).cpu().numpy())
+    scale = float(np.median(np.concatenate(ratios))) if ratios else 1.0
+    return pairs, scale

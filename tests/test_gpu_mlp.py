@@ -166,10 +166,46 @@ def test_learned_warm_start_gain_and_judge(bpf):
     Z = mlp.basis(16)
     Zh = Z.cpu().numpy()
     assert np.abs(Zh.T @ Zh - np.eye(16)).max() <= 1e-10
-    Xl, sl = learned.solve(A, Bd, N, mlp, Z, rtol=1e-8, itmax=100)
+    Xl, sl = learned.solve(A, Bd, N, mlp, Z, rtol=1e-8, itmax=100, judge="residual")
     assert sp_.solved and sl.solved
     assert np.linalg.norm(B - J @ Xl.cpu().numpy()) <= 1e-8 * nb * 1.01
     assert sl.niter <= sp_.niter, (sl.niter, sp_.niter)
+
+
+def test_learned_start_gains_on_held_out_operating_points(bpf):
+    """What the trained network gains over plain ILU(0) block-GMRES, on the solves the Newton
+    caller makes: sensitivities Gx^{-1} Gu[:, S] along a sequence of operating points of a
+    2,000-bus grid (3,798 unknowns; states perturbed by N(0, 0.001); 64 of the grid's 201 controls
+    per block).  The network is trained on 2,560 solver-generated solves at 40 points; at three
+    held-out points its judged warm start plus its rank-32 deflation basis take strictly fewer
+    iterations than the plain solve, and both reach 1e-8 of ||B||."""
+    import torch
+
+    from blockpowerflow_b200 import learned
+    from blockpowerflow_b200 import newton as NT
+
+    prob = NT.make_problem(bpf.grid.make_grid(2000, seed=0))
+    A = bpf.CuSparseMatrixCSR.from_scipy(prob.pattern)
+    N = bpf.ilu0(A, 64)
+    fam = learned.SensitivityFamily(prob, A, 64, sigma=0.001, seed=0)
+    pairs, scale = learned.family_pairs(fam, N, range(40))
+    assert len(pairs) == 40
+    mlp = learned.WarmStartMLP(A.n, hidden=512, seed=0)
+    mlp.set_scale(scale)
+    hist = learned.train(mlp, pairs, epochs=100, lr=3e-4, batch=64)
+    assert hist[-1] < 0.2 * hist[0], hist
+    Z = mlp.basis(32)
+    for t in (900, 901, 902):
+        B = fam.point(t)
+        N.refactor(A.nzVal)
+        nb = float(torch.linalg.norm(B))
+        Xp, sp_ = bpf.block_gmres(A, B, N=N, ldiv=True, restart=False, memory=300, atol=1e-8 * nb, rtol=0.0,
+                                  itmax=300)
+        Xl, sl = learned.solve(A, B, N, mlp, Z, rtol=1e-8, itmax=300)
+        assert sp_.solved and sl.solved
+        R = B - bpf.mul(A, Xl)
+        assert float(torch.linalg.norm(R)) <= 1e-8 * nb * 1.01
+        assert sl.niter < sp_.niter, (t, sl.niter, sp_.niter)
 
 
 # ---- deflated block-GMRES ---------------------------------------------------------------------
