@@ -520,6 +520,13 @@ def headline_batch(args, rank, world, dist):
                                       "SpMM 12 nnz + 4(n+1), the new block 8 n q x 14 passes, plus "
                                       "32 n q per basis block read (four CGS2 passes)")}
     tot = {k: int(v.sum()) for k, v in cyc.items()}
+    # the longest units (the makespan is at least the longest one)
+    top = np.argsort(cyc["total"])[::-1][:3]
+    longest = [{"system": int(mine[units["sys"][u]]), "n": int(mats[units["sys"][u]].shape[0]),
+                "q": int(units["q"][u]), "iterations": int(units["niter"][u]), "memory": int(units["memory"][u]),
+                "ms": float(cyc["total"][u]) / 1.965e6,
+                "phase_share": {k: round(float(cyc[k][u]) / max(float(cyc["total"][u]), 1.0), 3)
+                                for k in cyc if k != "total"}} for u in top]
     plan.close()
     if rank != 0:
         return
@@ -561,7 +568,8 @@ def headline_batch(args, rank, world, dist):
         "phase_share": {k: round(v / max(tot["total"], 1), 4) for k, v in tot.items() if k != "total"},
         "unit_cycles": {"max": int(cyc["total"].max()), "mean": float(cyc["total"].mean()),
                         "balanced_bound_ms": float(cyc["total"].sum()) / plan.grid / 1.965e6,
-                        "critical_path_ms": float(cyc["total"].max()) / 1.965e6},
+                        "critical_path_ms": float(cyc["total"].max()) / 1.965e6,
+                        "longest_units": longest},
         "autotune": {"seconds": t_tune, **{k: v for k, v in tune.items() if k != "cached"}},
         "plan_seconds": t_plan, "systems_this_rank": len(mine), "rhs_this_rank": my_rhs,
         "cpu_baseline": cb, "clocks": clocks,
@@ -939,6 +947,100 @@ def config_newton9k(args):
     print(json.dumps(line), flush=True)
 
 
+def config_learned70k(args):
+    """Fifth configuration: the learned warm start and rank-32 deflation basis on the 70,000-bus
+    grid (134,998 unknowns), 128 right-hand sides per block.  The right-hand sides are the Newton
+    caller's sensitivity solves (Gx X = Gu, benchmarks_nvidia.jl:29-39): at each operating point
+    of a sequence (states perturbed by N(0, 0.001)), 128 columns of Gu for controls drawn from a
+    fixed set of 512.  The network (3 layers, width 512, BF16 weights, FP32 accumulation) is trained
+    by the library's own tcgen05 kernels on the solver's solutions at `--train-points` points (160:
+    20,480 solves); at held-out points the learned solve (warm start + deflation, judged by plain
+    ILU(0) block-GMRES's stopping test) is timed against the plain solve, both to rtol 1e-8."""
+    import numpy as np
+    import torch
+
+    import blockpowerflow_b200 as bpf
+    from blockpowerflow_b200 import learned
+    from blockpowerflow_b200 import newton as NT
+
+    p, T = 128, args.train_points
+    t0 = time.time()
+    prob = NT.make_problem(bpf.grid.make_grid(70000, 5000, seed=0))
+    A = bpf.CuSparseMatrixCSR.from_scipy(prob.pattern)
+    n = A.n
+    N = bpf.ilu0(A, p)
+    fam = learned.SensitivityFamily(prob, A, p, sigma=0.001, seed=0)
+    t_setup = time.time() - t0
+    t0 = time.time()
+    pairs, scale = learned.family_pairs(fam, N, range(T), rtol=1e-8, itmax=400)
+    torch.cuda.synchronize()
+    t_data = time.time() - t0
+    t0 = time.time()
+    mlp = learned.WarmStartMLP(n, 512, seed=0)
+    mlp.set_scale(scale)
+    hist = learned.train(mlp, pairs, epochs=args.train_epochs, lr=3e-4, batch=128)
+    Z = mlp.basis(32)
+    torch.cuda.synchronize()
+    t_train = time.time() - t0
+    n_solves = sum(int(b.shape[1]) for b, _ in pairs)
+    del pairs
+    torch.cuda.empty_cache()
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        X, st = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return X, st, e0.elapsed_time(e1)
+
+    rows, errs = [], {}
+    held = list(range(10_000, 10_000 + max(3, args.steps)))
+    for k, t in enumerate(held):
+        B = fam.point(t)
+        nb = float(torch.linalg.norm(B))
+
+        def plain():
+            N.refactor(A.nzVal)
+            return bpf.block_gmres(A, B, N=N, ldiv=True, restart=False, memory=400, atol=1e-8 * nb, rtol=0.0,
+                                   itmax=400)
+
+        def learned_solve():
+            N.refactor(A.nzVal)
+            return learned.solve(A, B, N, mlp, Z, rtol=1e-8, itmax=400)
+
+        plain()   # warm-up of this point's shapes
+        Xp, sp_, ms_p = timed(plain)
+        Xl, sl, ms_l = timed(learned_solve)
+        rows.append({"point": t, "plain_iterations": sp_.niter, "learned_iterations": sl.niter,
+                     "plain_ms": ms_p, "learned_ms": ms_l, "plain_solved": bool(sp_.solved),
+                     "learned_solved": bool(sl.solved)})
+        if k == 0:   # the direct solve of one held-out point (SciPy sparse LU, FP64)
+            J = prob.pattern.copy()
+            J.data = A.nzVal.cpu().numpy()
+            Bh = B.cpu().numpy()
+            errs = {"plain": direct_error(J, Bh, Xp.cpu().numpy()), "learned": direct_error(J, Bh, Xl.cpu().numpy()),
+                    "relres_learned": rel_residual(J, Bh, Xl.cpu().numpy())}
+    ms_p = float(np.mean([r["plain_ms"] for r in rows]))
+    ms_l = float(np.mean([r["learned_ms"] for r in rows]))
+    line = {"config": {"workload": "grid70k_p128_learned_warm_start_rank32_deflation", "n_bus": 70000, "n_pv": 5000,
+                       "unknowns": n, "nnz": int(A.nnz), "rhs": p, "rtol": 1e-8,
+                       "rhs_family": "columns of Gu for 128 of a fixed set of 512 controls, at operating points "
+                                     "perturbed by N(0, 0.001)",
+                       "train_points": T, "held_out_points": len(held)},
+            "metric": "RHS solves/s at 1e-8 residual (learned vs plain ILU0 block-GMRES)", "unit": "RHS solves/s",
+            "value": p / (ms_l / 1e3), "plain_value": p / (ms_p / 1e3), "learned_over_plain": ms_p / ms_l,
+            "iterations": {"plain": [r["plain_iterations"] for r in rows],
+                           "learned": [r["learned_iterations"] for r in rows]},
+            "held_out": rows, "err_vs_direct": errs,
+            "training": {"solves": n_solves, "data_seconds": t_data, "train_seconds": t_train, "epochs": len(hist),
+                         "loss_first": hist[0], "loss_last": hist[-1], "setup_seconds": t_setup,
+                         "network": "3-layer MLP, width 512, BF16 weights with FP32 masters, tcgen05 GEMMs, Adam"},
+            "dtype": "f64 (network BF16)", "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
 def config_gmres9k(args, rank, world, dist):
     """The 9,000-bus grid of the second benchmark configuration (16,998 unknowns, ~121k nonzeros),
     64 Gaussian right-hand sides, block-GMRES with a right ILU(0), no restart (as in
@@ -1195,8 +1297,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--train-points", type=int, default=160, help="learned70k: training operating points")
+    ap.add_argument("--train-epochs", type=int, default=20, help="learned70k: training epochs")
     ap.add_argument("--config", default="batch512",
-                    choices=["batch512", "gmres9k", "gmres300", "bicgstab9k", "rf25k", "newton9k"],
+                    choices=["batch512", "gmres9k", "gmres300", "bicgstab9k", "rf25k", "newton9k", "learned70k"],
                     help="batch512 (default): the batched configuration; the others print one line "
                          "each for the other benchmark configurations")
     args = ap.parse_args()
@@ -1204,9 +1308,9 @@ def main():
         kernel_only(args.kernel_only, args.reps, args.iters, args.ordering, args.nsys, args.grid, args.p,
                     args.time)
         return
-    if args.config in ("gmres300", "bicgstab9k", "rf25k", "newton9k"):
-        {"gmres300": config_gmres300, "bicgstab9k": config_bicgstab9k,
-         "rf25k": config_rf25k, "newton9k": config_newton9k}[args.config](args)
+    if args.config in ("gmres300", "bicgstab9k", "rf25k", "newton9k", "learned70k"):
+        {"gmres300": config_gmres300, "bicgstab9k": config_bicgstab9k, "rf25k": config_rf25k,
+         "newton9k": config_newton9k, "learned70k": config_learned70k}[args.config](args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -152,7 +152,9 @@ class BatchPlan:
 
 
 # ---- autotuner ------------------------------------------------------------------------------
-CANDIDATES = [(slice_, cps) for slice_ in (8, 16, 32) for cps in (1, 2)]
+# One resident solve CTA per SM: the persistent kernel is compiled for one CTA per SM (all 255
+# registers a thread may hold, no spills), so ctas_per_sm = 2 runs as 1 and is not a candidate.
+CANDIDATES = [(slice_, 1) for slice_ in (8, 16, 32)]
 
 
 def batch_key(n, nrhs, device_name: str, extra: str = "") -> str:

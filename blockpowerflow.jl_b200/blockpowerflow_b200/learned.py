@@ -175,18 +175,33 @@ def judged_warm_start(mlp: WarmStartMLP, A: CuSparseMatrixCSR, B, N=None):
 
 def solve(A: CuSparseMatrixCSR, B, N, mlp: WarmStartMLP, Z=None, *, rtol: float = 1e-8,
           itmax: int = 300, judge: str = "error"):
-    """Right-preconditioned block-GMRES from the judged warm start, augmented with the learned
-    deflation basis Z (if given); the tolerance is rtol ||B||_F whatever the start.  judge:
-    "error" (the preconditioned residual, the default) or "residual" (judged_warm_start)."""
+    """Right-preconditioned block-GMRES from the network's warm start, augmented with the learned
+    deflation basis Z (if given); the tolerance is rtol ||B||_F whatever the start.
+
+    Plain ILU(0) block-GMRES is the judge and the fallback.  Up front, judged_warm_start keeps
+    the warm start only if it beats the zero start (judge "error": the estimated error through N,
+    the default; "residual": the residual; "final": always kept).  At the end, its stopping test
+    on ||B - A X||_F decides, and if the learned solve does not reach the tolerance within itmax
+    the plain solve from the zero start runs instead: the network can cost iterations, never
+    accuracy."""
     import torch
 
     from .krylov import block_gmres
 
     Bc = colmajor(B)
-    X0 = judged_warm_start(mlp, A, Bc, N if judge == "error" else None)
     nb = float(torch.linalg.norm(Bc))
-    return block_gmres(A, Bc, X0, N=N, ldiv=True, restart=False, memory=itmax, atol=rtol * nb,
-                       rtol=0.0, itmax=itmax, deflation=Z)
+    if judge == "final":
+        X0 = mlp.forward(Bc)
+    else:
+        X0 = judged_warm_start(mlp, A, Bc, N if judge == "error" else None)
+    X, st = block_gmres(A, Bc, X0, N=N, ldiv=True, restart=False, memory=itmax, atol=rtol * nb,
+                        rtol=0.0, itmax=itmax, deflation=Z)
+    if st.solved or (X0 is None and Z is None):
+        return X, st
+    Xp, sp_ = block_gmres(A, Bc, N=N, ldiv=True, restart=False, memory=itmax, atol=rtol * nb, rtol=0.0,
+                          itmax=itmax)
+    sp_.niter += st.niter   # the failed learned attempt counts
+    return Xp, sp_
 
 
 # ---- the sensitivity family: solves the Newton caller makes along a sequence of operating points

@@ -170,7 +170,7 @@ __device__ double cta_sum(double v, double *scratch) {
 template <int NT>
 __device__ void gram_t(const double *A, const double *B, int n, int q, double *red, double *dst, int ldd) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-    constexpr int UF = NT == 1 ? 16 : (NT == 2 ? 8 : 2);
+    constexpr int UF = NT == 1 ? 16 : (NT == 2 ? 8 : 4);
     constexpr int NC = NT <= 3 ? 2 : 1;   // independent accumulator chains (alternate k-steps)
     double acc[NC][NT][NT][2];
 #pragma unroll
@@ -250,7 +250,7 @@ template <int NT>
 __device__ void update_t(double *W, const double *A, size_t astr, const double *C, size_t cstr, int ldc,
                          int nb, int n, int q, double sign, bool init) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-    constexpr int MT = NT == 1 ? 8 : (NT == 2 ? 4 : (NT == 3 ? 2 : 1));
+    constexpr int MT = NT == 1 ? 8 : (NT == 2 ? 4 : (NT == 3 ? 4 : 2));
     constexpr int KK = 2 * NT;   // k-steps of 4 columns in a block of q <= 8 NT columns
     constexpr int RT = 8 * MT;
     for (int r0 = warp * RT; r0 < n; r0 += kW * RT) {
@@ -910,7 +910,7 @@ __device__ void solve_unit(const Sys &S, const Unit &U, const IO &io, const Cfg 
     }
 }
 
-__global__ void __launch_bounds__(kT, 2)
+__global__ void __launch_bounds__(kT, 1)
 batch_solve_kernel(const Sys *__restrict__ sys, const Unit *__restrict__ units, int nunits,
                    const IO *__restrict__ io, const int *__restrict__ sys_err, Cfg cfg, UnitOut *out,
                    int *counter) {

@@ -26,7 +26,7 @@ def test_autotune_runs_every_candidate_then_uses_the_cache(tmp_path):
     mats = [_Mat(500), _Mat(1200)]
     path = str(tmp_path / "tune.json")
     r = batch.autotune(mats, [8, 40], None, cache_path=path, runner=runner, device_name="dev")
-    assert (r["slice"], r["ctas_per_sm"]) == (16, 2) and not r["cached"]
+    assert (r["slice"], r["ctas_per_sm"]) == (16, 1) and not r["cached"]
     assert sorted(calls) == sorted(batch.CANDIDATES)
     data = json.load(open(path))
     assert len(data) == 1 and list(data.values())[0]["slice"] == 16

@@ -177,8 +177,8 @@ def test_learned_start_gains_on_held_out_operating_points(bpf):
     caller makes: sensitivities Gx^{-1} Gu[:, S] along a sequence of operating points of a
     2,000-bus grid (3,798 unknowns; states perturbed by N(0, 0.001); 64 of the grid's 201 controls
     per block).  The network is trained on 2,560 solver-generated solves at 40 points; at three
-    held-out points its judged warm start plus its rank-32 deflation basis take strictly fewer
-    iterations than the plain solve, and both reach 1e-8 of ||B||."""
+    held-out points the learned solve (its judged warm start and its rank-32 deflation basis)
+    takes strictly fewer iterations than the plain solve, and both reach 1e-8 of ||B||."""
     import torch
 
     from blockpowerflow_b200 import learned
