@@ -964,8 +964,9 @@ def config_learned70k(args):
     from blockpowerflow_b200 import newton as NT
 
     p, T = 128, args.train_points
+    nbus, npv = args.learned_buses, max(1, args.learned_buses // 14)
     t0 = time.time()
-    prob = NT.make_problem(bpf.grid.make_grid(70000, 5000, seed=0))
+    prob = NT.make_problem(bpf.grid.make_grid(nbus, npv, seed=0))
     A = bpf.CuSparseMatrixCSR.from_scipy(prob.pattern)
     n = A.n
     N = bpf.ilu0(A, p)
@@ -1024,7 +1025,8 @@ def config_learned70k(args):
                     "relres_learned": rel_residual(J, Bh, Xl.cpu().numpy())}
     ms_p = float(np.mean([r["plain_ms"] for r in rows]))
     ms_l = float(np.mean([r["learned_ms"] for r in rows]))
-    line = {"config": {"workload": "grid70k_p128_learned_warm_start_rank32_deflation", "n_bus": 70000, "n_pv": 5000,
+    line = {"config": {"workload": f"grid{nbus // 1000}k_p128_learned_warm_start_rank32_deflation", "n_bus": nbus,
+                       "n_pv": npv,
                        "unknowns": n, "nnz": int(A.nnz), "rhs": p, "rtol": 1e-8,
                        "rhs_family": "columns of Gu for 128 of a fixed set of 512 controls, at operating points "
                                      "perturbed by N(0, 0.001)",
@@ -1299,6 +1301,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--train-points", type=int, default=160, help="learned70k: training operating points")
     ap.add_argument("--train-epochs", type=int, default=20, help="learned70k: training epochs")
+    ap.add_argument("--learned-buses", type=int, default=70000, help="learned70k: grid size (70,000 buses)")
     ap.add_argument("--config", default="batch512",
                     choices=["batch512", "gmres9k", "gmres300", "bicgstab9k", "rf25k", "newton9k", "learned70k"],
                     help="batch512 (default): the batched configuration; the others print one line "

@@ -309,6 +309,28 @@ __device__ __noinline__ void update(double *W, const double *A, size_t astr, con
     }
 }
 
+// The same update with global coefficients C staged through shared memory `stage` (capacity
+// `cap` doubles) in chunks of blocks: every row tile of every warp reads each coefficient block,
+// so they come from shared memory (row stride q + 1, no bank conflicts) instead of L1 / L2.  W is
+// read and written once per chunk.  Collective: every thread of the CTA calls it.
+__device__ __noinline__ void update_staged(double *W, const double *A, size_t astr, const double *C, size_t cstr,
+                                           int nb, int n, int q, double sign, bool init, double *stage, int cap) {
+    const int lds = q + 1, per = q * lds;
+    const int chunk = max(1, cap / per);
+    for (int i0 = 0; i0 < nb; i0 += chunk) {
+        const int nc = min(chunk, nb - i0);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < nc * q * q; idx += kT) {
+            const int b = idx / (q * q), r = idx - b * q * q;
+            const int a = r / q, c = r - a * q;
+            stage[b * per + a * lds + c] = C[(size_t)(i0 + b) * cstr + (size_t)a * q + c];
+        }
+        __syncthreads();
+        update(W, A + (size_t)i0 * astr, astr, stage, per, lds, nc, n, q, sign, init || i0 > 0);
+    }
+    __syncthreads();
+}
+
 // ---------------------------------------------------------------------------------------
 // Sparse kernels: a group of 8 lanes per row (32 rows in flight per CTA), lane l holding
 // columns l, l + 8, ... (CPL of them) of the row-major block, the row's (column, value) pairs
@@ -833,12 +855,12 @@ __device__ void solve_unit(const Sys &S, const Unit &U, const IO &io, const Cfg 
             double *Rc = U.R + rcol_off(j, q);
             gram(U.V, bs, j + 1, Vn, n, q, sm.red, Rc, qq, q);
             pc.mark(PH_GRAM);
-            update(Vn, U.V, bs, Rc, qq, q, j + 1, n, q, -1.0, true);
+            update_staged(Vn, U.V, bs, Rc, qq, j + 1, n, q, -1.0, true, sm.red, kW * kLd * kLd);
             __syncthreads();
             pc.mark(PH_UPDATE);
             gram(U.V, bs, j + 1, Vn, n, q, sm.red, U.C2, qq, q);
             pc.mark(PH_GRAM);
-            update(Vn, U.V, bs, U.C2, qq, q, j + 1, n, q, -1.0, true);
+            update_staged(Vn, U.V, bs, U.C2, qq, j + 1, n, q, -1.0, true, sm.red, kW * kLd * kLd);
             __syncthreads();
             for (size_t idx = threadIdx.x; idx < (size_t)(j + 1) * qq; idx += kT) Rc[idx] += U.C2[idx];
             pc.mark(PH_UPDATE);
@@ -867,7 +889,7 @@ __device__ void solve_unit(const Sys &S, const Unit &U, const IO &io, const Cfg 
         if (j > 0) {
             backsub(U, j, sm);
             pc.mark(PH_BACKSUB);
-            update(U.Xh, U.Z, bs, U.g, qq, q, j, n, q, 1.0, true);
+            update_staged(U.Xh, U.Z, bs, U.g, qq, j, n, q, 1.0, true, sm.red, kW * kLd * kLd);
             __syncthreads();
             pc.mark(PH_UPDATE);
         }
