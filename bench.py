@@ -1011,7 +1011,8 @@ def config_learned70k(args):
             N.refactor(A.nzVal)
             return learned.solve(A, B, N, mlp, Z, rtol=1e-8, itmax=400)
 
-        plain()   # warm-up of this point's shapes
+        plain()           # warm-up of both paths at this point's shapes
+        learned_solve()
         Xp, sp_, ms_p = timed(plain)
         Xl, sl, ms_l = timed(learned_solve)
         rows.append({"point": t, "plain_iterations": sp_.niter, "learned_iterations": sl.niter,

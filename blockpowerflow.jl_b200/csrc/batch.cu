@@ -226,10 +226,84 @@ __device__ void gram_t(const double *A, const double *B, int n, int q, double *r
     __syncthreads();
 }
 
+// NB Gram products at once for narrow blocks (q <= 16): G_b = A_b^T B, A_b = A + b astr, in one
+// sweep over the rows (B's fragments loaded once for all NB blocks), so a narrow unit pays one
+// memory latency per NB basis blocks instead of one per block.  Partials of warp w, block b at
+// red + (w NB + b) 256 (ld 16).
+template <int NT, int NB>
+__device__ void gram_nb_t(const double *A, size_t astr, const double *B, int n, int q, double *red, double *dst,
+                          size_t dstr, int ldd) {
+    static_assert(NT <= 2 && NB * kW * 256 <= kW * kLd * kLd, "partials must fit the reduction area");
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    constexpr int UF = NT == 1 ? 16 : 8;
+    constexpr int NC = 2;
+    double acc[NB][NC][NT][NT][2];
+#pragma unroll
+    for (int k = 0; k < NB; k++)
+#pragma unroll
+        for (int h = 0; h < NC; h++)
+#pragma unroll
+            for (int a = 0; a < NT; a++)
+#pragma unroll
+                for (int b = 0; b < NT; b++) acc[k][h][a][b][0] = acc[k][h][a][b][1] = 0.0;
+    const int nks = (n + 3) >> 2;
+    for (int ks0 = warp * UF; ks0 < nks; ks0 += kW * UF) {
+        double af[NB][UF][NT], bf[UF][NT];
+#pragma unroll
+        for (int u = 0; u < UF; u++) {
+            const int r = (ks0 + u) * 4 + t;
+#pragma unroll
+            for (int i = 0; i < NT; i++) {
+                const int c = i * 8 + g;
+                const bool ok = r < n && c < q;
+                bf[u][i] = ok ? B[(size_t)r * q + c] : 0.0;
+#pragma unroll
+                for (int k = 0; k < NB; k++) af[k][u][i] = ok ? A[k * astr + (size_t)r * q + c] : 0.0;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NB; k++)
+#pragma unroll
+            for (int u = 0; u < UF; u++)
+#pragma unroll
+                for (int a = 0; a < NT; a++)
+#pragma unroll
+                    for (int b = 0; b < NT; b++)
+                        dmma(acc[k][u % NC][a][b][0], acc[k][u % NC][a][b][1], af[k][u][a], bf[u][b]);
+    }
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+        double *my = red + (warp * NB + k) * 256;
+#pragma unroll
+        for (int a = 0; a < NT; a++)
+#pragma unroll
+            for (int b = 0; b < NT; b++) {
+                my[(a * 8 + g) * 16 + b * 8 + 2 * t] = acc[k][0][a][b][0] + acc[k][1][a][b][0];
+                my[(a * 8 + g) * 16 + b * 8 + 2 * t + 1] = acc[k][0][a][b][1] + acc[k][1][a][b][1];
+            }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < NB * q * q; idx += kT) {
+        const int k = idx / (q * q), r = idx - k * q * q;
+        const int a = r / q, b = r - a * q;
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kW; w++) s += red[(w * NB + k) * 256 + a * 16 + b];
+        dst[k * dstr + a * ldd + b] = s;
+    }
+    __syncthreads();
+}
+
 // G_i = V_i^T W for i < nblk (V_i = V + i vstr) into dst + i dstr (ld ldd).
 __device__ __noinline__ void gram(const double *V, size_t vstr, int nblk, const double *W, int n, int q,
                                   double *red, double *dst, size_t dstr, int ldd) {
-    for (int i = 0; i < nblk; i++) {
+    int i = 0;
+    if (q <= 8) {
+        for (; i + 4 <= nblk; i += 4) gram_nb_t<1, 4>(V + i * vstr, vstr, W, n, q, red, dst + i * dstr, dstr, ldd);
+    } else if (q <= 16) {
+        for (; i + 2 <= nblk; i += 2) gram_nb_t<2, 2>(V + i * vstr, vstr, W, n, q, red, dst + i * dstr, dstr, ldd);
+    }
+    for (; i < nblk; i++) {
         switch ((q + 7) >> 3) {
             case 1: gram_t<1>(V + i * vstr, W, n, q, red, dst + i * dstr, ldd); break;
             case 2: gram_t<2>(V + i * vstr, W, n, q, red, dst + i * dstr, ldd); break;
@@ -263,7 +337,43 @@ __device__ void update_t(double *W, const double *A, size_t astr, const double *
                 acc[m][b][0] = (init && r < n && c < q) ? W[(size_t)r * q + c] : 0.0;
                 acc[m][b][1] = (init && r < n && c + 1 < q) ? W[(size_t)r * q + c + 1] : 0.0;
             }
-        for (int i = 0; i < nb; i++) {
+        int i0 = 0;
+        if constexpr (NT <= 2) {
+            // narrow blocks: two blocks' fragments loaded before their DMMAs (one memory
+            // latency per two blocks)
+            for (; i0 + 2 <= nb; i0 += 2) {
+                double bf[2][KK][NT], af[2][KK][MT];
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const double *Ai = A + (i0 + h) * astr;
+                    const double *Ci = C + (i0 + h) * cstr;
+#pragma unroll
+                    for (int k = 0; k < KK; k++) {
+                        const int kc = k * 4 + t;
+#pragma unroll
+                        for (int b = 0; b < NT; b++) {
+                            const int c = b * 8 + g;
+                            bf[h][k][b] = (kc < q && c < q) ? Ci[kc * ldc + c] : 0.0;
+                        }
+#pragma unroll
+                        for (int m = 0; m < MT; m++) {
+                            const int r = r0 + m * 8 + g;
+                            af[h][k][m] = (kc < q && r < n) ? Ai[(size_t)r * q + kc] : 0.0;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int h = 0; h < 2; h++)
+#pragma unroll
+                    for (int k = 0; k < KK; k++)
+#pragma unroll
+                        for (int m = 0; m < MT; m++)
+#pragma unroll
+                            for (int b = 0; b < NT; b++)
+                                dmma(acc[m][b][0], acc[m][b][1], sign * af[h][k][m], bf[h][k][b]);
+            }
+        }
+        for (int i = i0; i < nb; i++) {
             const double *Ai = A + i * astr;
             const double *Ci = C + i * cstr;
             double bf[KK][NT], af[KK][MT];
