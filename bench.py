@@ -632,6 +632,14 @@ def kernel_only(name, reps, iters=24, ordering="natural", nsys=64, kgrid="case70
         print(json.dumps({"kernel_only": name, "n": n, "p": P_RHS, "reps": reps, "loss": loss}))
         return
     J = bpf.grid.preset_jacobian(kgrid, 0)
+    if name == "spmm" and ordering.upper() == "RCM":
+        # the same matrix renumbered by reverse Cuthill-McKee (symmetric permutation), as a grid
+        # numbered with spatial locality would be: the rows that gather one row of X sit close
+        from scipy.sparse.csgraph import reverse_cuthill_mckee
+
+        perm = reverse_cuthill_mckee(J.tocsr(), symmetric_mode=False)
+        J = J.tocsr()[perm][:, perm].tocsr()
+        J.sort_indices()
     n = J.shape[0]
     p = kp
     A = bpf.CuSparseMatrixCSR.from_scipy(J)
