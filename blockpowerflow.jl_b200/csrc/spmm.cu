@@ -9,6 +9,9 @@
 //
 // Algorithmic bytes per launch: 12*nnz + 4*(n+1) + 8*n*p (X) + 8*n*p (Y written)
 // [+ 8*n*p when beta != 0 or the residual form reads B].
+#include <cstdint>
+#include <type_traits>
+
 #include "bpf_internal.cuh"
 
 namespace bpf {
@@ -73,6 +76,84 @@ spmm_rm_kernel(int n, const int *__restrict__ rp, const int *__restrict__ ci,
     }
 }
 
+// Blocks of 64, 128, ... columns: a warp per row, lane l holding columns 2l, 2l + 1 (+ 64 j) as
+// one 16-byte load per gathered row segment, half the load instructions of the 8-byte form and
+// twice the bytes each one brings; eight entries' loads in flight.  Same products and summation
+// order per output as spmm_rm_kernel.
+template <int C2>
+__global__ void __launch_bounds__(256)
+spmm_rm2_kernel(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                const double *__restrict__ av, int base, int p, double alpha,
+                const double *__restrict__ X, double beta, double *__restrict__ Y,
+                const double *__restrict__ Bres, const int *gate) {
+    __shared__ int s_off;
+    if (threadIdx.x == 0) s_off = (gate && *gate == 0) ? 1 : 0;
+    __syncthreads();
+    if (s_off) return;
+    const int lane = threadIdx.x & 31;
+    const int warps = blockDim.x >> 5;
+    for (int row = blockIdx.x * warps + (threadIdx.x >> 5); row < n; row += gridDim.x * warps) {
+        double2 acc[C2];
+#pragma unroll
+        for (int j = 0; j < C2; j++) acc[j] = make_double2(0.0, 0.0);
+        const int rs = __ldg(rp + row) - base, re = __ldg(rp + row + 1) - base;
+        for (int kb = rs; kb < re; kb += 32) {
+            const int k = kb + lane;
+            int c = 0;
+            double a = 0.0;
+            if (k < re) {
+                c = __ldg(ci + k) - base;
+                a = __ldg(av + k);
+            }
+            const int cnt = min(32, re - kb);
+#pragma unroll 8
+            for (int t = 0; t < cnt; t++) {
+                const int ct = __shfl_sync(0xffffffffu, c, t);
+                const double at = __shfl_sync(0xffffffffu, a, t);
+                const double2 *xr = reinterpret_cast<const double2 *>(X + (size_t)ct * p);
+#pragma unroll
+                for (int j = 0; j < C2; j++) {
+                    const double2 v = __ldg(xr + lane + 32 * j);
+                    acc[j].x += at * v.x;
+                    acc[j].y += at * v.y;
+                }
+            }
+        }
+        double2 *yr = reinterpret_cast<double2 *>(Y + (size_t)row * p);
+#pragma unroll
+        for (int j = 0; j < C2; j++) {
+            double2 v;
+            if (Bres) {
+                const double2 b = reinterpret_cast<const double2 *>(Bres + (size_t)row * p)[lane + 32 * j];
+                v = make_double2(b.x - acc[j].x, b.y - acc[j].y);
+            } else {
+                v = make_double2(alpha * acc[j].x, alpha * acc[j].y);
+                if (beta != 0.0) {
+                    const double2 y0 = yr[lane + 32 * j];
+                    v.x += beta * y0.x;
+                    v.y += beta * y0.y;
+                }
+            }
+            yr[lane + 32 * j] = v;
+        }
+    }
+}
+
+template <int C2>
+static bpf_status launch_spmm2(bpf_ctx *ctx, int n, long long nnz, const int *rp, const int *ci,
+                               const double *av, int base, int p, double alpha, const double *X,
+                               double beta, double *Y, const double *B, const int *gate) {
+    const int threads = 256, rows_per_block = threads / 32;
+    int blocks = (int)std::min<long long>(ceil_div(n, rows_per_block), (long long)ctx->num_sms * 16);
+    if (blocks < 1) blocks = 1;
+    const double np = (double)n * p;
+    const double bytes = 12.0 * nnz + 4.0 * (n + 1) + 8.0 * np + 8.0 * np + ((B || beta != 0.0) ? 8.0 * np : 0.0);
+    KScope ks(ctx, BPF_KC_SPMM, bytes, 2.0 * nnz * p);
+    spmm_rm2_kernel<C2><<<blocks, threads, 0, ctx->stream>>>(n, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+    BPF_LAUNCHED(ctx);
+    return BPF_SUCCESS;
+}
+
 template <int G, int CPL, typename TX>
 static bpf_status launch_spmm(bpf_ctx *ctx, int n, long long nnz, const int *rp, const int *ci,
                               const double *av, int base, int p, double alpha, const TX *X,
@@ -97,6 +178,17 @@ static bpf_status spmm_dispatch(bpf_ctx *ctx, int n, long long nnz, const int *r
                                 const double *av, int base, int p, double alpha, const TX *X,
                                 double beta, double *Y, const double *B, const int *gate) {
     if (n == 0 || p == 0) return BPF_SUCCESS;
+    if constexpr (std::is_same<TX, double>::value) {
+        // 16-byte rows: p a multiple of 64 and every block 16-byte aligned
+        const bool aligned = ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(Y) |
+                               reinterpret_cast<uintptr_t>(B)) & 15) == 0;
+        if (aligned && p % 64 == 0 && p <= 256) {
+            if (p == 64) return launch_spmm2<1>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+            if (p == 128) return launch_spmm2<2>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+            if (p == 192) return launch_spmm2<3>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+            return launch_spmm2<4>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
+        }
+    }
     if (p <= 4) return launch_spmm<4, 1>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
     if (p <= 8) return launch_spmm<8, 1>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
     if (p <= 16) return launch_spmm<16, 1>(ctx, n, nnz, rp, ci, av, base, p, alpha, X, beta, Y, B, gate);
