@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -156,16 +157,26 @@ bpf_status prec_setup(bpf_ctx *ctx, int kind, int n, const std::vector<int> &rp,
                     : build_tri(n, rp.data(), ci.data(), diag.data(), 1, false);
     std::vector<int> pp;
     PairVec pdst, psrc;
-    const bool pairs_ok = build_pairs(n, rp.data(), ci.data(), diag.data(), ic, pp, pdst, psrc);
+    const char *env_pl = getenv("BPF_LU_PAIRLESS");
+    const bool force_pairless = kind == PREC_LU && env_pl && atoi(env_pl) != 0;
+    const bool pairs_ok = !force_pairless && build_pairs(n, rp.data(), ci.data(), diag.data(), ic, pp, pdst, psrc);
     P->npairs = (long long)pdst.size();
     auto fail = [&](bpf_status s) {
         cudaStreamSynchronize(ctx->stream);
         bpf_prec_destroy(P);
         return s;
     };
-    if (!pairs_ok)
+    if (!pairs_ok && kind != PREC_LU)
         return fail(set_error(ctx, BPF_ERR_NOT_SUPPORTED,
                               "factorization update pairs exceed 2^31 - 1 (pattern of %d entries too dense)", nnz));
+    if (!pairs_ok) {
+        // the LU refactorization finds each L entry's updates by a search in its row instead
+        P->pairless = true;
+        long long upd = 0;
+        for (int i = 0; i < n; i++)
+            for (int q = rp[i]; q < diag[i]; q++) upd += rp[ci[q] + 1] - diag[ci[q]] - 1;
+        P->npairs = upd;
+    }
     bpf_status s;
     if ((s = tri_upload(ctx, lo, P->lower)) != BPF_SUCCESS) return fail(s);
     if ((s = tri_upload(ctx, up, P->upper)) != BPF_SUCCESS) return fail(s);
@@ -216,6 +227,15 @@ bpf_status prec_setup(bpf_ctx *ctx, int kind, int n, const std::vector<int> &rp,
         P->cl_max_level = mx;
         up_i(&P->cl_lev_ptr, lptr);
         up_i(&P->cl_ent, ent);
+        if (P->pairless) {
+            std::vector<int> erow(ent.size());
+            std::vector<int> rowof(nnz > 0 ? nnz : 1);
+            for (int i = 0; i < n; i++)
+                for (int q = rp[i]; q < rp[i + 1]; q++) rowof[q] = i;
+            for (size_t t = 0; t < ent.size(); t++) erow[t] = rowof[ent[t]];
+            up_i(&P->cl_row, erow);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        }
         // push lists of the two sweeps: forward, L entry (i, k) leaves row k (level of k in
         // the forward sweep) for row i; backward, U entry (i, k), i < k, leaves row k for row i
         int pmx = 0;
@@ -616,6 +636,7 @@ bpf_status bpf_prec_destroy(bpf_prec *P) {
     cudaFree(P->sf_flags);
     cudaFree(P->cl_lev_ptr);
     cudaFree(P->cl_ent);
+    cudaFree(P->cl_row);
     cudaFree(P->bj_rows);
     cudaFree(P->bj_blk);
     cudaFree(P->bj_loc);

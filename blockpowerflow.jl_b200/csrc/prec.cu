@@ -429,6 +429,61 @@ __global__ void __launch_bounds__(256) lu_colstep_kernel(int nlev, const int *__
     }
 }
 
+// The same column steps without stored update pairs: for the L entry e = (i, k) (row i from
+// erow), every U entry (k, j), j > k, updates (i, j), whose position is found by a binary search
+// of column j in row i after e (the fill pattern is closed under elimination, so it is there).
+// Used where the pairs would exceed 2^31 - 1 (the 70,000-bus minimum-degree LU).
+__global__ void __launch_bounds__(256) lu_colstep_search_kernel(int nlev, const int *__restrict__ lev_ptr,
+                                                                const int *__restrict__ ent,
+                                                                const int *__restrict__ erow,
+                                                                const int *__restrict__ rp,
+                                                                const int *__restrict__ ci,
+                                                                const int *__restrict__ diag, double *fv,
+                                                                DevStatus *ds) {
+    __shared__ unsigned s_gen;
+    if (threadIdx.x == 0) s_gen = barrier_gen_start(ds);
+    __syncthreads();
+    unsigned gen = s_gen;
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    for (int l = 0; l < nlev; l++) {
+        const int q0 = __ldg(lev_ptr + l), q1 = __ldg(lev_ptr + l + 1);
+        for (int q = q0 + gw; q < q1; q += nw) {
+            const int e = __ldg(ent + q);
+            const int i = __ldg(erow + q);
+            const int k = __ldg(ci + e);
+            double lik = 0.0;
+            if (lane == 0) {
+                const double piv = __ldcg(fv + __ldg(diag + k));
+                if (piv == 0.0) {
+                    if (atomicCAS(&ds->err, 0, (int)DEV_ZERO_PIVOT) == 0) ds->aux = k;
+                } else {
+                    lik = __ldcg(fv + e) / piv;
+                }
+                fv[e] = lik;
+            }
+            lik = __shfl_sync(0xffffffffu, lik, 0);
+            if (lik == 0.0) continue;
+            const int u0 = __ldg(diag + k) + 1, u1 = __ldg(rp + k + 1);
+            const int r0 = e + 1, r1 = __ldg(rp + i + 1);
+            for (int t = u0 + lane; t < u1; t += 32) {
+                const int j = __ldg(ci + t);
+                int lo = r0, hi = r1;   // first position in [r0, r1) with column >= j
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (__ldg(ci + mid) < j) lo = mid + 1;
+                    else hi = mid;
+                }
+                if (lo < r1 && __ldg(ci + lo) == j) atomicAdd(fv + lo, -lik * __ldcg(fv + t));
+            }
+        }
+        if (l + 1 < nlev) {
+            if (!grid_barrier(ds, gen)) return;
+        }
+    }
+}
+
 // LU solve in push form, in place on row-major n x p blocks (p <= 256): forward sweep, level by
 // level, a warp per unit-L entry (i, k) whose source row k is final: y_i -= l_ik y_k; backward
 // sweep, a warp per U entry (i, k), i < k: y_i -= (u_ik / u_kk) y_k with y_k not yet divided;
@@ -483,6 +538,23 @@ static bpf_status coop_grid(bpf_ctx *ctx, K kernel, int threads, size_t smem, in
 }
 
 bpf_status factor_numeric(bpf_ctx *ctx, bpf_prec *P) {
+    if (P->kind == PREC_LU && P->cl_nlev > 0 && P->pairless) {
+        int grid = 1;
+        BPF_TRY(coop_grid(ctx, lu_colstep_search_kernel, 256, 0, std::max(1, ceil_div(P->cl_max_level, 8)), &grid));
+        int nlev = P->cl_nlev;
+        const int *lp = P->cl_lev_ptr, *en = P->cl_ent, *er = P->cl_row, *rp = P->rp, *ci = P->ci, *dg = P->diag;
+        double *fv = P->fv;
+        DevStatus *ds = ctx->dstat;
+        void *args[] = {&nlev, (void *)&lp, (void *)&en, (void *)&er, (void *)&rp, (void *)&ci, (void *)&dg, &fv, &ds};
+        // Algorithmic bytes: the factor values read and written once, the entry lists, and per
+        // update a column index, a value read and one atomically updated (the search's reads of
+        // row i are cached re-reads)
+        KScope ks(ctx, BPF_KC_FACTOR, 16.0 * P->nnz + 8.0 * (P->n + 1) + 28.0 * P->npairs, 2.0 * P->npairs);
+        BPF_CUDA(ctx, cudaLaunchCooperativeKernel((const void *)lu_colstep_search_kernel, dim3(grid), dim3(256),
+                                                  args, 0, ctx->stream));
+        BPF_LAUNCHED(ctx);
+        return BPF_SUCCESS;
+    }
     if (P->kind == PREC_LU && P->cl_nlev > 0) {
         int grid = 1;
         BPF_TRY(coop_grid(ctx, lu_colstep_kernel, 256, 0, std::max(1, ceil_div(P->cl_max_level, 8)), &grid));

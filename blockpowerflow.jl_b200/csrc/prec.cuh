@@ -116,6 +116,11 @@ struct bpf_prec {
     // row k or column k.  cl_lev_ptr / cl_ent: the L entries of each level's steps.
     int cl_nlev = 0, cl_max_level = 0;
     int *cl_lev_ptr = nullptr, *cl_ent = nullptr;
+    // Without stored update pairs (patterns whose pairs exceed 2^31 - 1, or BPF_LU_PAIRLESS=1):
+    // each L entry's updates are found by a search in its row; cl_row = the row of each listed
+    // entry.  npairs then counts the updates.
+    bool pairless = false;
+    int *cl_row = nullptr;
     // LU solves in push form (right-looking): per level of each sweep, the factor entries whose
     // source row became final at that level, as (source row, target row, position in fv).
     int ps_nlev[2] = {0, 0}, ps_max_level = 0;
