@@ -452,23 +452,35 @@ function deflation_basis(M::WarmStartMLP, rank::Int; seed::Integer=0)
     return Z
 end
 
-# the network's warm start if its residual ||B - A X0|| is below ||B|| (the zero start's), else nothing
-function judged_warm_start(M::WarmStartMLP, A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64})
+# The network's warm start if it beats the zero start, else nothing.  Without N: the residual,
+# ||B - A X0|| < ||B||.  With the right preconditioner N: the estimated error,
+# ||N \ (B - A X0)|| < ||N \ B|| (the network's misses are short-wavelength components that A
+# amplifies in the residual and the preconditioner removes).
+function judged_warm_start(M::WarmStartMLP, A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64}, N=nothing)
     X0 = warm_start(M, B)
     R = copy(B)
     check(ccall((:bpf_spmm, libbpf), Cint,
                 (Ptr{Cvoid}, Ref{CsrDesc}, Cint, Cdouble, CuPtr{Cdouble}, Cint, Cdouble, CuPtr{Cdouble}, Cint),
                 ctx(), Ref(desc(A)), size(X0, 2), -1.0, pointer(X0), stride(X0, 2), 1.0, pointer(R), stride(R, 2)))
-    return norm(R) < norm(B) ? X0 : nothing
+    N === nothing && return norm(R) < norm(B) ? X0 : nothing
+    E = similar(B)
+    ldiv!(E, N, R)
+    e0 = norm(E)
+    ldiv!(E, N, B)
+    return e0 < norm(E) ? X0 : nothing
 end
 
 # right-preconditioned block-GMRES from the judged warm start, with the deflation basis Z if given;
-# tolerance rtol ||B||_F whatever the start
+# tolerance rtol ||B||_F whatever the start; if it does not reach it within itmax, the plain solve
+# from the zero start runs instead (the network can cost iterations, never accuracy)
 function learned_solve(A::CuSparseMatrixCSR{Float64,Cint}, B::CuMatrix{Float64}, N, M::WarmStartMLP;
                        Z::Union{Nothing,CuMatrix{Float64}}=nothing, rtol::Float64=1e-8, itmax::Int=300)
-    X0 = judged_warm_start(M, A, B)
-    return block_gmres(A, B, X0; N=N, ldiv=true, restart=false, memory=itmax, atol=rtol * norm(B),
-                       rtol=0.0, itmax=itmax, deflation=Z)
+    X0 = judged_warm_start(M, A, B, N)
+    X, st = block_gmres(A, B, X0; N=N, ldiv=true, restart=false, memory=itmax, atol=rtol * norm(B),
+                        rtol=0.0, itmax=itmax, deflation=Z)
+    (st.solved || (X0 === nothing && Z === nothing)) && return X, st
+    return block_gmres(A, B; N=N, ldiv=true, restart=false, memory=itmax, atol=rtol * norm(B),
+                       rtol=0.0, itmax=itmax)
 end
 
 # ---- householder (src/block_utils.jl:38-53) ----------------------------------------------

@@ -346,7 +346,8 @@ typedef struct {
     int factor_dtype;   /* BPF_F32 (default: FP32 factors, flexible FP64 outer) or BPF_F64 */
     int ordering;       /* BPF_ORDER_AMD (default, minimum degree), _MDQ, _RCM or _NATURAL */
     int slice;          /* widest column slice q, 1..32; 0 -> 16 */
-    int ctas_per_sm;    /* resident solve CTAs per SM, 1 or 2; 0 -> 2 */
+    int ctas_per_sm;    /* resident solve CTAs per SM asked for, 1 or 2 (0 -> 2); the solve
+                           kernel holds 255 registers per thread, so one CTA per SM runs */
 } bpf_batch_opts;
 BPF_API void bpf_batch_opts_default(bpf_batch_opts *opts);
 /* Analyse nsys systems (A[s]: device CSR, FP64; nrhs[s] >= 1 columns) and capture the solve
