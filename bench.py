@@ -1340,7 +1340,10 @@ def main():
             import torch
 
             torch.cuda.set_device(local)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        # the reference arm's rank 0 runs minutes of CPU work while the other ranks wait at the
+        # final barrier; the GPU arm's ranks meet within seconds of each other
+        wait_s = 3600 if args.impl == "reference" else 600
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=wait_s))
     try:
         if args.impl == "reference":
             (run_reference_batch if args.config == "batch512" else run_reference)(args, rank, world)
