@@ -16,6 +16,13 @@
  *   - orc_lu_*             host LU + refactor-on-fixed-pivots + solve (src/cusolverRF.jl:56-331),
  *                          dense, for the small cases the oracle has to finish in seconds.
  *
+ * Pinning (tests/test_oracle.py, fixtures from the reference's data by tests/golden/make_golden.py):
+ * the RF routines against the reference's four cusolverRF known-answer tests (test/cusolverRF.jl),
+ * ILU(0) / IC(0) against exact factorizations on patterns without fill, the Householder QR
+ * against LAPACK's conventions.  The block solvers are pinned to the reference tests' settings
+ * and to the direct solve only: their iteration counts and histories are parity unpinned, since
+ * the reference's block-solver tests only print and the reference cannot run here (no Julia).
+ *
  * Dense blocks are column-major with an explicit leading dimension, like Julia matrices.
  * CSR arrays are 0-based int32.  Parallelism (OpenMP) only splits independent loops
  * (rows of a SpMM, RHS columns of a triangular solve, columns of a reflector update) so the
