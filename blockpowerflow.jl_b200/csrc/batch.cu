@@ -72,7 +72,8 @@ struct Unit {
     double *Xh;   // the solution slice in A_hat's order
     double *R;    // Hessenberg column blocks: column j holds blocks 0..j+1 at (j(j+3)/2) q^2
     double *C2;   // (m + 1) q x q: second Gram-Schmidt pass coefficients
-    double *HV;   // reflectors: column j at j (q + 2) q: v_c[t] at t q + c, tau_c at (q + 1) q + c
+    double *HV;   // reflectors: column j at j (2 q + 2) q: v_c[t] at t q + c, tau_c at (q + 1) q + c,
+                  // the compact-WY factor T (q x q, upper) at (q + 2) q + r q + c
     double *g;    // (m + 1) q x q: least-squares right-hand side (then y)
     double est;   // estimated cost (host ordering)
 };
@@ -784,6 +785,60 @@ __device__ void store_blk(double *dst, const double *src, int q, bool upper_only
     }
 }
 
+// Compact-WY factor of the window's reflector set (`refl` as house_window leaves it): with
+// Y = [v_0 .. v_{q-1}] (v_c on window rows c .. c + q, v_c[0] = 1), H_0 H_1 .. H_{q-1} =
+// I - Y T Y^T, T upper triangular: T_cc = tau_c, T[0:c, c] = -tau_c T[0:c, 0:c] (Y^T v_c)[0:c]
+// (LAPACK's forward, columnwise larft).  T into `T` (ld kLd); z is q doubles of scratch.
+__device__ void wy_factor(const double *refl, int q, double *T, double *z) {
+    for (int idx = threadIdx.x; idx < q * kLd; idx += kT) T[idx] = 0.0;
+    __syncthreads();
+    for (int c = 0; c < q; c++) {
+        const double tau = refl[(kQ + 1) * kLd + c];
+        // z_r = v_r . v_c over the rows they share, c .. r + q (r < c)
+        for (int r = threadIdx.x; r < c; r += kT) {
+            double acc = 0.0;
+            for (int row = c; row <= r + q; row++) acc += refl[(row - r) * kLd + r] * refl[(row - c) * kLd + c];
+            z[r] = acc;
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < c; r += kT) {
+            double acc = 0.0;
+            for (int u = r; u < c; u++) acc += T[r * kLd + u] * z[u];
+            T[r * kLd + c] = -tau * acc;
+        }
+        if (threadIdx.x == 0) T[c * kLd + c] = tau;
+        __syncthreads();
+    }
+}
+
+// The window (top; bot) <- H_{q-1} .. H_0 (top; bot) = (I - Y T^T Y^T)(top; bot) in three
+// products (W1 = Y^T X, W2 = T^T W1, X -= Y W2) instead of q reflector steps.
+__device__ void wy_apply(double *top, double *bot, const double *refl, const double *T, double *W1, double *W2,
+                         int q) {
+    for (int idx = threadIdx.x; idx < q * q; idx += kT) {
+        const int r = idx / q, b = idx - r * q;
+        double acc = 0.0;
+        for (int t = 0; t <= q; t++) acc += refl[t * kLd + r] * win_at(top, bot, q, r + t, b);
+        W1[r * kLd + b] = acc;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < q * q; idx += kT) {
+        const int r = idx / q, b = idx - r * q;
+        double acc = 0.0;
+        for (int u = 0; u <= r; u++) acc += T[u * kLd + r] * W1[u * kLd + b];
+        W2[r * kLd + b] = acc;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < 2 * q * q; idx += kT) {
+        const int row = idx / q, b = idx - row * q;
+        const int r0 = max(0, row - q), r1 = min(q - 1, row);
+        double acc = 0.0;
+        for (int r = r0; r <= r1; r++) acc += refl[(row - r) * kLd + r] * W2[r * kLd + b];
+        win_at(top, bot, q, row, b) -= acc;
+    }
+    __syncthreads();
+}
+
 // Column j of the block Hessenberg matrix (blocks 0..j+1 in U.R) -> R column j; new reflectors
 // into U.HV; g_j, g_{j+1} updated.  Returns ||g_{j+1}||_F, the least-squares residual.
 __device__ double hess_update(const Unit &U, int j, Smem &sm) {
@@ -793,19 +848,24 @@ __device__ double hess_update(const Unit &U, int j, Smem &sm) {
     double *wa = sm.red, *wb = sm.red + kQ * kLd;
     double *refl = sm.red + 2 * kQ * kLd;
     double *ga = refl + (kQ + 2) * kLd, *gb = ga + kQ * kLd;
+    double *Tw = gb + kQ * kLd, *zw = Tw + kQ * kLd;   // WY factor of a window, larft scratch
+    const size_t hvs = (size_t)(2 * q + 2) * q;
     load_blk(wa, Rc, q);
     __syncthreads();
     double *top = wa, *bot = wb;
     for (int i = 0; i < j; i++) {
         load_blk(bot, Rc + (i + 1) * qq, q);
-        const double *hv = U.HV + (size_t)i * (q + 2) * q;
+        const double *hv = U.HV + (size_t)i * hvs;
         for (int idx = threadIdx.x; idx < (q + 1) * q; idx += kT) {
             const int t = idx / q, c = idx - t * q;
             refl[t * kLd + c] = hv[idx];
         }
-        for (int c = threadIdx.x; c < q; c += kT) refl[(kQ + 1) * kLd + c] = hv[(q + 1) * q + c];
+        for (int idx = threadIdx.x; idx < q * q; idx += kT) {
+            const int r = idx / q, c = idx - r * q;
+            Tw[r * kLd + c] = hv[(q + 2) * q + idx];
+        }
         __syncthreads();
-        refl_apply_all(top, bot, refl, q);
+        wy_apply(top, bot, refl, Tw, ga, gb, q);   // ga / gb are free until the window loop ends
         store_blk(Rc + i * qq, top, q, false);
         __syncthreads();
         double *tmp = top;
@@ -815,12 +875,17 @@ __device__ double hess_update(const Unit &U, int j, Smem &sm) {
     load_blk(bot, Rc + (j + 1) * qq, q);
     __syncthreads();
     house_window(top, bot, refl, q);
-    double *hv = U.HV + (size_t)j * (q + 2) * q;
+    wy_factor(refl, q, Tw, zw);
+    double *hv = U.HV + (size_t)j * hvs;
     for (int idx = threadIdx.x; idx < (q + 1) * q; idx += kT) {
         const int t = idx / q, c = idx - t * q;
         hv[idx] = refl[t * kLd + c];
     }
     for (int c = threadIdx.x; c < q; c += kT) hv[(q + 1) * q + c] = refl[(kQ + 1) * kLd + c];
+    for (int idx = threadIdx.x; idx < q * q; idx += kT) {
+        const int r = idx / q, c = idx - r * q;
+        hv[(q + 2) * q + idx] = Tw[r * kLd + c];
+    }
     store_blk(Rc + j * qq, top, q, true);
     load_blk(ga, U.g + j * qq, q);
     for (int idx = threadIdx.x; idx < q * q; idx += kT) {
@@ -1190,7 +1255,7 @@ int auto_memory(int n, int q) {
 size_t unit_doubles(int n, int q, int m) {
     const size_t bs = (size_t)n * q, qq = (size_t)q * q;
     return bs * (2 * (size_t)m + 3) + qq * ((size_t)m * (m + 3) / 2 + 2 * ((size_t)m + 1)) +
-           (size_t)m * (q + 2) * q;
+           (size_t)m * (2 * q + 2) * q;
 }
 
 struct Packer {
