@@ -14,6 +14,9 @@ Outputs (committed, a few hundred KB):
                    Jacobian and dense sensitivity right-hand sides, benchmarks_nvidia.jl:29-39)
                    with the direct solution of Gx X = Gu.
   dump_case118.npz the same for case118 (a second real grid).
+  gx_case9241pegase.npz  benchmarks/dump/Gx_case9241pegase.mtx alone (17,036 x 17,036, 129k
+                   nonzeros: the Jacobian benchmarks_nvidia.jl solves by default, :22); the tests
+                   draw their own right-hand sides and direct solutions.
 """
 import os
 import sys
@@ -51,6 +54,8 @@ def main(ref_root):
         Gu = np.asarray(mmread(os.path.join(ref_root, "benchmarks", "dump", f"Gu_{case}.mtx")).todense())
         Xd = spl.splu(Gx.tocsc()).solve(Gu)
         np.savez_compressed(os.path.join(HERE, f"dump_{case}.npz"), **csr_arrays(Gx), Gu=Gu, X=Xd)
+    Gx = sp.csr_matrix(mmread(os.path.join(ref_root, "benchmarks", "dump", "Gx_case9241pegase.mtx")))
+    np.savez_compressed(os.path.join(HERE, "gx_case9241pegase.npz"), **csr_arrays(Gx))
     print("wrote fixtures to", HERE)
 
 

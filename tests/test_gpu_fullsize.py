@@ -13,6 +13,8 @@ library itself:
     <= 1e-8; FP64 factors solved to rtol 1e-11, every X within 1e-9 of the direct solve (some
     systems stagnate at the rounding floor of their true residual, above 1e-11).
 """
+import os
+
 import numpy as np
 import pytest
 import scipy.sparse.linalg as spla
@@ -153,3 +155,33 @@ def test_grid70k_rf_without_stored_pairs_against_direct(bpf):
     assert _rel(X.cpu().numpy(), Xd) <= np.sqrt(np.finfo(float).eps)
     Xr = rf.solve_refined(A, Bt, steps=1)
     assert _rel(Xr.cpu().numpy(), Xd) <= 1e-10
+
+
+def test_real_case9241pegase_block_gmres_against_direct_and_oracle(bpf, oracle_lib):
+    """The Jacobian the reference's benchmark solves by default (benchmarks_nvidia.jl:22,
+    Gx_case9241pegase: 17,036 unknowns, 129k nonzeros), 64 seeded Gaussian right-hand sides,
+    block-GMRES + natural-order FP64 ILU(0), unrestarted: the iteration count within one of the
+    oracle's, the true residual <= 1e-8 at rtol 1e-8, and X within 1e-10 of the direct solve at
+    rtol 1e-13."""
+    import torch
+
+    from conftest import load_csr
+
+    J, _ = load_csr("gx_case9241pegase.npz")
+    n = J.shape[0]
+    B = bpf.grid.gaussian_rhs(n, 64, 11)
+    A = bpf.CuSparseMatrixCSR.from_scipy(J)
+    N = bpf.ilu0(A, 64)
+    Bt = torch.as_tensor(B, device="cuda")
+    X, st = bpf.block_gmres(A, Bt, N=N, ldiv=True, restart=False, memory=300, atol=0.0, rtol=1e-8,
+                            itmax=300)
+    assert st.solved
+    assert np.linalg.norm(B - J @ X.cpu().numpy()) / np.linalg.norm(B) <= 1e-8
+    O = oracle_lib
+    O.set_threads(os.cpu_count() or 1)
+    _, so = O.block_gmres(J, B, N=(1, O.ilu0(J)), memory=300, restart=False, atol=0.0, rtol=1e-8, itmax=300)
+    assert so.solved and abs(st.niter - so.niter) <= 1, (st.niter, so.niter)
+    X, st = bpf.block_gmres(A, Bt, N=N, ldiv=True, restart=False, memory=300, atol=0.0, rtol=1e-13,
+                            itmax=300)
+    assert st.solved, st
+    assert _rel(X.cpu().numpy(), _direct(J, B)) <= 1e-10

@@ -151,3 +151,13 @@ def test_oracle_on_benchmark_dump(dump300, oracle_lib):
                           itmax=600)
     assert st.solved
     np.testing.assert_allclose(X, z["X"][:, :32], rtol=0, atol=1e-8 * np.abs(z["X"]).max())
+
+
+def test_real_case9241pegase_fixture():
+    """The committed Gx_case9241pegase fixture (tests/golden/make_golden.py) is the reference's
+    benchmark Jacobian: 17,036 x 17,036 with 129,412 nonzeros, square, every diagonal present."""
+    from conftest import load_csr
+
+    J, _ = load_csr("gx_case9241pegase.npz")
+    assert J.shape == (17036, 17036) and J.nnz == 129412
+    assert np.all(J.diagonal() != 0)
