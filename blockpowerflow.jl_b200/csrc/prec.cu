@@ -787,8 +787,34 @@ trsv_sf_kernel(TriKernelArgs t0, TriKernelArgs t1, int p, const double *X, doubl
         const TF *dinv = std::is_same<TF, float>::value ? (const TF *)t.dinvf : (const TF *)t.dinv;
         const unsigned want = 2u * epoch + (unsigned)phase;   // ready word of a row this sweep reads
         double *Y = phase == 0 ? Zf : Yout;                     // the sweep's solved rows
+        // the next position's row id, entry range and first 32 entries are loaded while the
+        // current row waits and gathers (they do not depend on any row's result)
+        int nx_i = 0, nx_rs = 0, nx_re = 0, nx_c = 0;
+        TF nx_a = (TF)0;
+        if (wid < t.n) {
+            nx_i = __ldg(t.rows + wid);
+            nx_rs = __ldg(t.rp + wid);
+            nx_re = __ldg(t.rp + wid + 1);
+            if (nx_rs + lane < nx_re) {
+                nx_c = __ldg(t.ci + nx_rs + lane);
+                nx_a = __ldg(val + nx_rs + lane);
+            }
+        }
         for (int q = wid; alive && q < t.n; q += nw) {
-            const int i = __ldg(t.rows + q);
+            const int i = nx_i, rs = nx_rs, re = nx_re;
+            const int c0 = nx_c;
+            const TF a0 = nx_a;
+            if (q + nw < t.n) {
+                nx_i = __ldg(t.rows + q + nw);
+                nx_rs = __ldg(t.rp + q + nw);
+                nx_re = __ldg(t.rp + q + nw + 1);
+                nx_c = 0;
+                nx_a = (TF)0;
+                if (nx_rs + lane < nx_re) {
+                    nx_c = __ldg(t.ci + nx_rs + lane);
+                    nx_a = __ldg(val + nx_rs + lane);
+                }
+            }
             const int io = perm ? __ldg(perm + i) : i;   // row of i in the caller's order
             TF acc[CPL];
 #pragma unroll
@@ -801,15 +827,14 @@ trsv_sf_kernel(TriKernelArgs t0, TriKernelArgs t1, int p, const double *X, doubl
                     acc[j] = (TF)0;
                 }
             }
-            const int rs = __ldg(t.rp + q), re = __ldg(t.rp + q + 1);
             for (int kb = rs; kb < re; kb += 32) {
                 const int k = kb + lane;
                 int c = 0;
                 TF a = (TF)0;
                 bool ok = true;
                 if (k < re) {
-                    c = __ldg(t.ci + k);
-                    a = __ldg(val + k);
+                    c = kb == rs ? c0 : __ldg(t.ci + k);
+                    a = kb == rs ? a0 : __ldg(val + k);
                     // bounded wait for row c of this sweep (acquire polls: measured faster than
                     // relaxed polls followed by one acquire fence, 92 vs 105 us at 9,000 buses)
                     long long it = 0;
