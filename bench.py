@@ -8,8 +8,8 @@ right-hand sides each (18,919 in all), every system solved by ILU(0)-preconditio
 numeric factorization of every system + the solve of every right-hand side; the pattern analysis
 is set-up (a Newton loop pays it once per pattern).
 
-  value : the batched path (FP32 ILU(0) factors in minimum-degree order, FP64 residual and
-          orthogonalization, launch shape from the autotuner): one CUDA-graph launch per step,
+  value : the batched path (FP32 ILU(0) factors, FP64 residual and orthogonalization, launch
+          shape and fill-reducing order from the autotuner): one CUDA-graph launch per step,
           device-resident blocks, CUDA events around each step (max over ranks), per-kernel
           instrumentation off, L2 flushed between steps.
   plain_fp64_dropin : the reference's call per system, block_gmres(A, B; N=ilu0(A, p), ldiv=true)
@@ -378,7 +378,8 @@ def headline_batch(args, rank, world, dist):
     tune = bpf.autotune(dm, nrhs, Bd, cache_path=os.environ.get("BPF_TUNE_CACHE"), repeats=1)
     t_tune = time.time() - t0
     t0 = time.time()
-    plan = bpf.BatchPlan(dm, nrhs, slice=tune["slice"], ctas_per_sm=tune["ctas_per_sm"])
+    plan = bpf.BatchPlan(dm, nrhs, slice=tune["slice"], ctas_per_sm=tune["ctas_per_sm"],
+                         ordering=tune["ordering"], slices=tune["slices"])
     torch.cuda.synchronize()
     t_plan = time.time() - t0
     Xd = [bpf.empty_colmajor(A.shape[0], p, dev) for A, p in zip(mats, nrhs)]
@@ -546,9 +547,13 @@ def headline_batch(args, rank, world, dist):
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f64 (FP32 ILU0 factors)", "data": "synthetic", "config": cfg_all,
         "method": {"value": "batched: one CUDA-graph launch per step (ILU0 kernel + persistent block-GMRES "
-                            "kernel), FP32 ILU0 factors in minimum-degree order, FP64 SpMM / orthogonalization / "
-                            "Hessenberg least squares / X, flexible GMRES, autotuned launch shape",
-                   "slice": tune["slice"], "ctas_per_sm": tune["ctas_per_sm"], "units": plan.nunits,
+                            "kernel), FP32 ILU0 factors in the autotuned fill-reducing order, FP64 SpMM / "
+                            "orthogonalization / Hessenberg least squares / X, flexible GMRES, autotuned "
+                            "launch shape",
+                   "slice": tune["slice"], "ctas_per_sm": tune["ctas_per_sm"],
+                   "ordering": {"AMD": "minimum degree", "RCM": "reverse Cuthill-McKee"}.get(
+                       tune["ordering"], tune["ordering"]),
+                   "narrowed_systems": int(sum(1 for v in (tune["slices"] or []) if v)), "units": plan.nunits,
                    "grid": plan.grid},
         "all_solved": all_ok, "max_relres": max_rel,
         "err_vs_direct": {"max": max_err, "median": float(np.median([r["err"] for r in R])),
@@ -577,7 +582,7 @@ def headline_batch(args, rank, world, dist):
     print(json.dumps(line), flush=True)
 
 
-def kernel_only(name, reps, iters=24, ordering="natural", nsys=64, kgrid="case70k", kp=128, timed=False):
+def kernel_only(name, reps, iters=24, ordering=None, nsys=64, kgrid="case70k", kp=128, timed=False):
     """A few launches of one kernel on a case whose blocks exceed L2, for ncu captures:
     70,000-bus grid (134,998 unknowns, ~980k nonzeros), 128 right-hand sides."""
     import numpy as np
@@ -585,20 +590,35 @@ def kernel_only(name, reps, iters=24, ordering="natural", nsys=64, kgrid="case70
 
     import blockpowerflow_b200 as bpf
 
+    if name != "batch":
+        ordering = ordering or "natural"
     if name == "batch":
-        # `reps` solves of the first `nsys` systems of the batched configuration (the launch
-        # shape the autotuner picks for the full batch: slice 32, one CTA per SM); nsys = 512 is
-        # the whole batch
+        # `reps` solves of the first `nsys` systems of the batched configuration; nsys = 512 is
+        # the whole batch.  The plan is the one the default run's autotuner chose when its cache
+        # (BPF_TUNE_CACHE, written by that run) holds this batch, so that no tuning launch
+        # precedes the captured ones; else the shape it picks for the full batch (slice 32, one
+        # CTA per SM, reverse Cuthill-McKee)
         _, nrhs, mats, Bs = batch_workload(systems=range(nsys))
         nrhs = nrhs[:nsys]
         dm = [bpf.CuSparseMatrixCSR.from_scipy(A) for A in mats]
         Bd = [bpf.colmajor(torch.as_tensor(B, device="cuda")) for B in Bs]
-        plan = bpf.BatchPlan(dm, nrhs, slice=32, ctas_per_sm=1)
+        tune = {"slice": 32, "ctas_per_sm": 1, "ordering": ordering or "RCM", "slices": None, "cached": False}
+        cache = os.environ.get("BPF_TUNE_CACHE")
+        if cache and ordering is None:
+            key = bpf.batch.batch_key([A.n for A in dm], nrhs, torch.cuda.get_device_name(),
+                                      bpf.batch.cache_extra(bpf.batch.CANDIDATES, "AMD"))
+            hit = bpf.batch.load_cache(cache).get(key)
+            if hit:
+                tune = {**hit, "cached": True}
+        plan = bpf.BatchPlan(dm, nrhs, slice=tune["slice"], ctas_per_sm=tune["ctas_per_sm"],
+                             ordering=tune["ordering"], slices=tune["slices"])
         for _ in range(reps):
             Xs, st = plan.solve(Bd)
         torch.cuda.synchronize()
         print(json.dumps({"kernel_only": name, "systems": nsys, "rhs": int(sum(nrhs)), "reps": reps,
                           "solved": all(s.solved for s in st), "units": plan.nunits,
+                          "plan": {k: tune[k] for k in ("slice", "ordering", "cached")},
+                          "narrowed_systems": int(sum(1 for v in (tune["slices"] or []) if v)),
                           "device_bytes": plan.device_bytes}))
         plan.close()
         return
@@ -1298,7 +1318,8 @@ def main():
                     default=None, help="launch one kernel a few times on a small case (for ncu)")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--iters", type=int, default=24, help="block-GMRES iterations (--kernel-only gmres)")
-    ap.add_argument("--ordering", default="natural", help="ILU(0) ordering (--kernel-only gmres)")
+    ap.add_argument("--ordering", default=None,
+                    help="ILU(0) ordering of --kernel-only (default: natural; RCM for batch)")
     ap.add_argument("--nsys", type=int, default=64, help="systems of the batch (--kernel-only batch)")
     ap.add_argument("--grid", default="case70k", help="preset grid of --kernel-only trsv/spmm/factor/gram")
     ap.add_argument("--p", type=int, default=128, help="right-hand sides of --kernel-only trsv/spmm")

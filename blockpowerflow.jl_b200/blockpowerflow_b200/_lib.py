@@ -130,6 +130,7 @@ SIGNATURES = {
     "bpf_rf_destroy": (_I, [_P]),
     "bpf_batch_opts_default": (None, [C.POINTER(BatchOpts)]),
     "bpf_batch_plan": (_I, [_P, _I, _P, _P, C.POINTER(BatchOpts), C.POINTER(_P)]),
+    "bpf_batch_plan_sliced": (_I, [_P, _I, _P, _P, _P, C.POINTER(BatchOpts), C.POINTER(_P)]),
     "bpf_batch_solve": (_I, [_P, _P, _P, _P, _P, _P]),
     "bpf_batch_unit_stats": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "bpf_batch_unit_cycles": (_I, [_P, _P]),

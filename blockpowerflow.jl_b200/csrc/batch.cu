@@ -1304,9 +1304,18 @@ bpf_status bpf_batch_destroy(bpf_batch *b) {
 
 bpf_status bpf_batch_plan(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A, const int *nrhs,
                           const bpf_batch_opts *opts_in, bpf_batch **out) {
+    return bpf_batch_plan_sliced(ctx, nsys, A, nrhs, nullptr, opts_in, out);
+}
+
+bpf_status bpf_batch_plan_sliced(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A, const int *nrhs,
+                                 const int *slices, const bpf_batch_opts *opts_in, bpf_batch **out) {
     if (!ctx || !out) return BPF_ERR_INVALID_VALUE;
     *out = nullptr;
     if (nsys <= 0 || !A || !nrhs) return set_error(ctx, BPF_ERR_INVALID_VALUE, "batch: nsys > 0, A and nrhs required");
+    if (slices)
+        for (int s = 0; s < nsys; s++)
+            if (slices[s] < 0 || slices[s] > kQ)
+                return set_error(ctx, BPF_ERR_INVALID_VALUE, "batch: slices[%d] must be 0..%d", s, kQ);
     bpf_batch_opts o;
     if (opts_in) o = *opts_in;
     else bpf_batch_opts_default(&o);
@@ -1420,7 +1429,7 @@ bpf_status bpf_batch_plan(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A, const i
         // wider than n / 24 exhausts the Krylov space of a small system within a few iterations,
         // where a partial breakdown (directions that have converged) stalls block-GMRES
         const int p = nrhs[s];
-        const int qs = std::max(1, std::min(qmax, n / 24));
+        const int qs = std::max(1, std::min(slices && slices[s] > 0 ? slices[s] : qmax, n / 24));
         const int ns = (p + qs - 1) / qs;
         int col = 0;
         for (int k = 0; k < ns; k++) {

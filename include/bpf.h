@@ -354,6 +354,13 @@ BPF_API void bpf_batch_opts_default(bpf_batch_opts *opts);
  * graph.  A[s].vals is re-read by every solve: new values on the same pattern go in place. */
 BPF_API bpf_status bpf_batch_plan(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A, const int *nrhs,
                                   const bpf_batch_opts *opts, bpf_batch **batch);
+/* bpf_batch_plan with a widest column slice per system: slices[s] in 1..32, or 0 for
+ * opts->slice (slices NULL: opts->slice for every system).  Narrower slices for the systems
+ * whose units take longest shorten the critical path of the persistent solve (its makespan is
+ * at least its longest unit). */
+BPF_API bpf_status bpf_batch_plan_sliced(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A,
+                                         const int *nrhs, const int *slices,
+                                         const bpf_batch_opts *opts, bpf_batch **batch);
 /* X[s] (n_s x nrhs[s], column-major, ld ldx[s]) = A[s] \ B[s] for every s; B, X, ldb, ldx are
  * HOST arrays of nsys entries (device block pointers; ldb / ldx NULL -> n_s).  stats (nsys
  * entries, nullable): niter = the most iterations of the system's units, solved = all units

@@ -197,9 +197,40 @@ def test_autotune_times_candidates_and_caches(bpf, tmp_path):
     path = str(tmp_path / "tune.json")
     r = bpf.autotune(dm, nrhs, Bd, cache_path=path, candidates=[(8, 2), (16, 2), (32, 1)], repeats=1)
     assert not r["cached"] and (r["slice"], r["ctas_per_sm"]) in [(8, 2), (16, 2), (32, 1)]
+    assert r["ordering"] == "AMD"
     assert all(ok for _, ok in r["timings"].values())
     r2 = bpf.autotune(dm, nrhs, Bd, cache_path=path, candidates=[(8, 2), (16, 2), (32, 1)])
     assert r2["cached"] and r2["slice"] == r["slice"]
+    # the default candidates time both fill-reducing orders; the choice builds a plan that solves
+    r3 = bpf.autotune(dm, nrhs, Bd, repeats=1)
+    assert set(r3["timings"]) == {f"{s}x{c}x{o}" for s, c, o in bpf.batch.CANDIDATES}
+    plan = bpf.BatchPlan(dm, nrhs, slice=r3["slice"], ctas_per_sm=r3["ctas_per_sm"], ordering=r3["ordering"])
+    Xs, st = plan.solve(Bd)
+    assert all(s.solved for s in st)
+    for A, B, X in zip(mats, Bs, Xs):
+        assert np.linalg.norm(B - A @ X.cpu().numpy()) <= 1.01e-8 * np.linalg.norm(B)
+    plan.close()
+
+
+def test_batch_per_system_slices(bpf):
+    """bpf_batch_plan_sliced: a widest slice per system (0 keeps the plan's), each system's
+    columns still covered exactly once, every system at the tolerance."""
+    mats = _systems(bpf, [300, 800, 1500], seed0=120)
+    nrhs = [20, 9, 40]
+    Bs = _rhs(bpf, mats, nrhs, seed=21)
+    plan, Xs, st, dm = _solve(bpf, mats, Bs, nrhs, slice=32, slices=[0, 3, 8])
+    u = plan.unit_stats()
+    widest = {s: max(q for q, ss in zip(u["q"], u["sys"]) if ss == s) for s in range(3)}
+    assert widest == {0: 20, 1: 3, 2: 8}
+    for s, (A, B, X) in enumerate(zip(mats, Bs, Xs)):
+        assert st[s].solved, (s, st[s])
+        assert np.linalg.norm(B - A @ X) / np.linalg.norm(B) <= 1e-8 * 1.01, s
+        assert sum(q for q, ss in zip(u["q"], u["sys"]) if ss == s) == nrhs[s]
+    plan.close()
+    with pytest.raises(bpf.BPFError):
+        bpf.BatchPlan(dm, nrhs, slices=[0, 33, 0])
+    with pytest.raises(bpf.DimensionMismatch):
+        bpf.BatchPlan(dm, nrhs, slices=[0, 3])
 
 
 def test_batch_wide_blocks_on_small_systems_converge(bpf):

@@ -107,9 +107,10 @@ def _batch_solve(bpf, mats, Bs, nrhs, **kw):
         plan.close()
 
 
-def test_batch512_fp32_factors_every_system_meets_the_tolerance(bpf, batch512):
+@pytest.mark.parametrize("ordering", ["AMD", "RCM"])
+def test_batch512_fp32_factors_every_system_meets_the_tolerance(bpf, batch512, ordering):
     _, nrhs, mats, Bs = batch512
-    Xs, st = _batch_solve(bpf, mats, Bs, nrhs)
+    Xs, st = _batch_solve(bpf, mats, Bs, nrhs, ordering=ordering)
     for s, (A, B, X) in enumerate(zip(mats, Bs, Xs)):
         assert st[s].solved, (s, st[s])
         assert np.linalg.norm(B - A @ X) / np.linalg.norm(B) <= 1e-8 * (1 + 1e-9), s
