@@ -295,9 +295,172 @@ __device__ void gram_nb_t(const double *A, size_t astr, const double *B, int n, 
     __syncthreads();
 }
 
+// Gram products of blocks whose width q = 8 F + R has a thin rim (R columns past F full 8-wide
+// tiles): the F x F full tiles on the DMMA pipe, the rim (G[0:8F, 8F:q], G[8F:q, 0:8F] and the
+// R x R corner) with FP64 FMAs, instead of padding q to 8 (F + 1) columns, whose DMMA work is
+// (F + 1)^2 / F^2 of the full tiles' (4x at q = 9).  Used for R = 1 (q = 9, 17, 25): measured
+// on the 512-grid batch, the longest units with q = 9 and 17 ran 5 % faster; with R = 2 and 3
+// the rim's loads and FMAs cost more than the padding they save (units with q = 26, 27 slower).  Lane (g, t) holds rows r_t of
+// column 8 i + g of every full tile, as for the DMMA fragments, and loads the rim values of its
+// row itself (the same cache lines); its rim partials are summed over t by shuffles, and over
+// the warps through shared memory as the tiles are.  NB blocks A_b = A + b astr per sweep (the
+// new block's fragments loaded once for all of them); partials of warp w, block b at
+// red + (w NB + b) ld^2, ld = kLd for NB = 1 and 16 otherwise (q <= 16 then).
+template <int F, int R, int NB>
+__device__ void gram_rim_t(const double *A, size_t astr, const double *B, int n, int q, double *red,
+                           double *dst, size_t dstr, int ldd) {
+    constexpr int LD = NB == 1 ? kLd : 16;
+    static_assert(8 * F + R <= LD && NB * kW * LD * LD <= kW * kLd * kLd, "partials must fit the reduction area");
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    constexpr int UF = (F == 1 && NB == 1) ? 8 : (F * NB <= 2 ? 4 : 2);
+    constexpr int NC = F <= 2 ? 2 : 1;
+    double acc[NB][NC][F][F][2];
+    double ra[NB][F][R], rb[NB][F][R], rc[NB][R][R];
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+#pragma unroll
+        for (int h = 0; h < NC; h++)
+#pragma unroll
+            for (int a = 0; a < F; a++)
+#pragma unroll
+                for (int b = 0; b < F; b++) acc[k][h][a][b][0] = acc[k][h][a][b][1] = 0.0;
+#pragma unroll
+        for (int i = 0; i < F; i++)
+#pragma unroll
+            for (int r = 0; r < R; r++) ra[k][i][r] = rb[k][i][r] = 0.0;
+#pragma unroll
+        for (int r = 0; r < R; r++)
+#pragma unroll
+            for (int c = 0; c < R; c++) rc[k][r][c] = 0.0;
+    }
+    const int nks = (n + 3) >> 2;
+    for (int ks0 = warp * UF; ks0 < nks; ks0 += kW * UF) {
+        double af[NB][UF][F], bf[UF][F], ar[NB][UF][R], br[UF][R];
+#pragma unroll
+        for (int u = 0; u < UF; u++) {
+            const int r = (ks0 + u) * 4 + t;
+            const bool ok = r < n;
+            const size_t ro = (size_t)r * q;
+#pragma unroll
+            for (int i = 0; i < F; i++) {
+                bf[u][i] = ok ? B[ro + i * 8 + g] : 0.0;
+#pragma unroll
+                for (int k = 0; k < NB; k++) af[k][u][i] = ok ? A[k * astr + ro + i * 8 + g] : 0.0;
+            }
+#pragma unroll
+            for (int c = 0; c < R; c++) {
+                br[u][c] = ok ? B[ro + 8 * F + c] : 0.0;
+#pragma unroll
+                for (int k = 0; k < NB; k++) ar[k][u][c] = ok ? A[k * astr + ro + 8 * F + c] : 0.0;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NB; k++)
+#pragma unroll
+            for (int u = 0; u < UF; u++) {
+#pragma unroll
+                for (int a = 0; a < F; a++)
+#pragma unroll
+                    for (int b = 0; b < F; b++)
+                        dmma(acc[k][u % NC][a][b][0], acc[k][u % NC][a][b][1], af[k][u][a], bf[u][b]);
+#pragma unroll
+                for (int i = 0; i < F; i++)
+#pragma unroll
+                    for (int c = 0; c < R; c++) {
+                        ra[k][i][c] = fma(af[k][u][i], br[u][c], ra[k][i][c]);
+                        rb[k][i][c] = fma(ar[k][u][c], bf[u][i], rb[k][i][c]);
+                    }
+#pragma unroll
+                for (int r = 0; r < R; r++)
+#pragma unroll
+                    for (int c = 0; c < R; c++) rc[k][r][c] = fma(ar[k][u][r], br[u][c], rc[k][r][c]);
+            }
+    }
+    // rim partials: sum over the four row lanes t of each g
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+#pragma unroll
+        for (int i = 0; i < F; i++)
+#pragma unroll
+            for (int c = 0; c < R; c++) {
+                ra[k][i][c] += __shfl_xor_sync(0xffffffffu, ra[k][i][c], 1);
+                ra[k][i][c] += __shfl_xor_sync(0xffffffffu, ra[k][i][c], 2);
+                rb[k][i][c] += __shfl_xor_sync(0xffffffffu, rb[k][i][c], 1);
+                rb[k][i][c] += __shfl_xor_sync(0xffffffffu, rb[k][i][c], 2);
+            }
+#pragma unroll
+        for (int r = 0; r < R; r++)
+#pragma unroll
+            for (int c = 0; c < R; c++) {
+                rc[k][r][c] += __shfl_xor_sync(0xffffffffu, rc[k][r][c], 1);
+                rc[k][r][c] += __shfl_xor_sync(0xffffffffu, rc[k][r][c], 2);
+            }
+        double *my = red + (warp * NB + k) * LD * LD;
+#pragma unroll
+        for (int a = 0; a < F; a++)
+#pragma unroll
+            for (int b = 0; b < F; b++) {
+                double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                for (int h = 0; h < NC; h++) {
+                    s0 += acc[k][h][a][b][0];
+                    s1 += acc[k][h][a][b][1];
+                }
+                my[(a * 8 + g) * LD + b * 8 + 2 * t] = s0;
+                my[(a * 8 + g) * LD + b * 8 + 2 * t + 1] = s1;
+            }
+        if (t == 0) {
+#pragma unroll
+            for (int i = 0; i < F; i++)
+#pragma unroll
+                for (int c = 0; c < R; c++) {
+                    my[(i * 8 + g) * LD + 8 * F + c] = ra[k][i][c];
+                    my[(8 * F + c) * LD + i * 8 + g] = rb[k][i][c];
+                }
+            if (g == 0) {
+#pragma unroll
+                for (int r = 0; r < R; r++)
+#pragma unroll
+                    for (int c = 0; c < R; c++) my[(8 * F + r) * LD + 8 * F + c] = rc[k][r][c];
+            }
+        }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < NB * q * q; idx += kT) {
+        const int k = idx / (q * q), rr = idx - k * q * q;
+        const int a = rr / q, b = rr - a * q;
+        double sum = 0.0;
+#pragma unroll
+        for (int w = 0; w < kW; w++) sum += red[(w * NB + k) * LD * LD + a * LD + b];
+        dst[k * dstr + a * ldd + b] = sum;
+    }
+    __syncthreads();
+}
+
+template <int R>
+__device__ __forceinline__ void gram_rim(const double *V, size_t vstr, int nblk, const double *W, int n, int q,
+                                         double *red, double *dst, size_t dstr, int ldd) {
+    const int F = q >> 3;
+    int i = 0;
+    if (F == 1) {
+        for (; i + 2 <= nblk; i += 2) gram_rim_t<1, R, 2>(V + i * vstr, vstr, W, n, q, red, dst + i * dstr, dstr, ldd);
+    }
+    for (; i < nblk; i++) {
+        switch (F) {
+            case 1: gram_rim_t<1, R, 1>(V + i * vstr, vstr, W, n, q, red, dst + i * dstr, dstr, ldd); break;
+            case 2: gram_rim_t<2, R, 1>(V + i * vstr, vstr, W, n, q, red, dst + i * dstr, dstr, ldd); break;
+            default: gram_rim_t<3, R, 1>(V + i * vstr, vstr, W, n, q, red, dst + i * dstr, dstr, ldd); break;
+        }
+    }
+}
+
 // G_i = V_i^T W for i < nblk (V_i = V + i vstr) into dst + i dstr (ld ldd).
 __device__ __noinline__ void gram(const double *V, size_t vstr, int nblk, const double *W, int n, int q,
                                   double *red, double *dst, size_t dstr, int ldd) {
+    if (q > 8 && q < 32 && (q & 7) == 1) {
+        gram_rim<1>(V, vstr, nblk, W, n, q, red, dst, dstr, ldd);
+        return;
+    }
     int i = 0;
     if (q <= 8) {
         for (; i + 4 <= nblk; i += 4) gram_nb_t<1, 4>(V + i * vstr, vstr, W, n, q, red, dst + i * dstr, dstr, ldd);
@@ -410,8 +573,142 @@ __device__ void update_t(double *W, const double *A, size_t astr, const double *
     }
 }
 
+// The block update for widths q = 8 F + R with a thin rim (used for R = 1): the F x F full tiles of
+// every block product on the DMMA pipe (2 F k-steps), the rim with FP64 FMAs instead of padding q
+// to 8 (F + 1): the K rim (columns 8F .. q of A_i times rows 8F .. q of C_i) into the full output
+// tiles, and the output rim (columns 8F .. q of W) as per-lane partial dot products over the
+// lane's k-steps (k = t mod 4, the DMMA A-fragment layout) plus the corner terms of k = 8F + t,
+// summed over the four lanes t of a row by shuffles after the last block.  Every lane has loaded
+// its rows of A before any lane stores (the shuffles order them), so W may be A itself (nb = 1,
+// init = false), as in update_t.
+template <int F, int R>
+__device__ void update_rim_t(double *W, const double *A, size_t astr, const double *C, size_t cstr, int ldc,
+                             int nb, int n, int q, double sign, bool init) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    constexpr int MT = F == 1 ? 4 : 2;
+    constexpr int KK = 2 * F;
+    constexpr int RT = 8 * MT;
+    for (int r0 = warp * RT; r0 < n; r0 += kW * RT) {
+        double acc[MT][F][2], pr[MT][R];
+#pragma unroll
+        for (int m = 0; m < MT; m++) {
+            const int r = r0 + m * 8 + g;
+#pragma unroll
+            for (int b = 0; b < F; b++) {
+                const int c = b * 8 + 2 * t;
+                acc[m][b][0] = (init && r < n) ? W[(size_t)r * q + c] : 0.0;
+                acc[m][b][1] = (init && r < n) ? W[(size_t)r * q + c + 1] : 0.0;
+            }
+#pragma unroll
+            for (int c = 0; c < R; c++) pr[m][c] = 0.0;
+        }
+        for (int i = 0; i < nb; i++) {
+            const double *Ai = A + i * astr;
+            const double *Ci = C + i * cstr;
+            double bf[KK][F], af[KK][MT], ar[MT][R];
+#pragma unroll
+            for (int k = 0; k < KK; k++) {
+                const int kc = k * 4 + t;
+#pragma unroll
+                for (int b = 0; b < F; b++) bf[k][b] = Ci[kc * ldc + b * 8 + g];
+#pragma unroll
+                for (int m = 0; m < MT; m++) {
+                    const int r = r0 + m * 8 + g;
+                    af[k][m] = r < n ? Ai[(size_t)r * q + kc] : 0.0;
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < MT; m++) {
+                const int r = r0 + m * 8 + g;
+#pragma unroll
+                for (int c = 0; c < R; c++) ar[m][c] = r < n ? sign * Ai[(size_t)r * q + 8 * F + c] : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < KK; k++)
+#pragma unroll
+                for (int m = 0; m < MT; m++)
+#pragma unroll
+                    for (int b = 0; b < F; b++) dmma(acc[m][b][0], acc[m][b][1], sign * af[k][m], bf[k][b]);
+            // K rim into the full tiles: rows 8F + c of C_i
+#pragma unroll
+            for (int c = 0; c < R; c++) {
+                const double *crow = Ci + (8 * F + c) * ldc + 2 * t;
+#pragma unroll
+                for (int b = 0; b < F; b++) {
+                    const double c0 = crow[b * 8], c1 = crow[b * 8 + 1];
+#pragma unroll
+                    for (int m = 0; m < MT; m++) {
+                        acc[m][b][0] = fma(ar[m][c], c0, acc[m][b][0]);
+                        acc[m][b][1] = fma(ar[m][c], c1, acc[m][b][1]);
+                    }
+                }
+            }
+            // output rim: this lane's k-steps (columns 4 k + t of A_i) and corner row 8F + t
+#pragma unroll
+            for (int c = 0; c < R; c++) {
+#pragma unroll
+                for (int k = 0; k < KK; k++) {
+                    const double cv = Ci[(k * 4 + t) * ldc + 8 * F + c];
+#pragma unroll
+                    for (int m = 0; m < MT; m++) pr[m][c] = fma(sign * af[k][m], cv, pr[m][c]);
+                }
+                if (t < R) {
+                    const double cv = Ci[(8 * F + t) * ldc + 8 * F + c];
+#pragma unroll
+                    for (int m = 0; m < MT; m++) {
+                        double a = 0.0;
+#pragma unroll
+                        for (int e = 0; e < R; e++)
+                            if (e == t) a = ar[m][e];
+                        pr[m][c] = fma(a, cv, pr[m][c]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < MT; m++)
+#pragma unroll
+            for (int c = 0; c < R; c++) {
+                pr[m][c] += __shfl_xor_sync(0xffffffffu, pr[m][c], 1);
+                pr[m][c] += __shfl_xor_sync(0xffffffffu, pr[m][c], 2);
+            }
+#pragma unroll
+        for (int m = 0; m < MT; m++) {
+            const int r = r0 + m * 8 + g;
+            if (r >= n) continue;
+#pragma unroll
+            for (int b = 0; b < F; b++) {
+                const int c = b * 8 + 2 * t;
+                W[(size_t)r * q + c] = acc[m][b][0];
+                W[(size_t)r * q + c + 1] = acc[m][b][1];
+            }
+            if (t == 0) {
+#pragma unroll
+                for (int c = 0; c < R; c++) {
+                    double *w = W + (size_t)r * q + 8 * F + c;
+                    *w = (init ? *w : 0.0) + pr[m][c];
+                }
+            }
+        }
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void update_rim(double *W, const double *A, size_t astr, const double *C, size_t cstr,
+                                           int ldc, int nb, int n, int q, double sign, bool init) {
+    switch (q >> 3) {
+        case 1: update_rim_t<1, R>(W, A, astr, C, cstr, ldc, nb, n, q, sign, init); break;
+        case 2: update_rim_t<2, R>(W, A, astr, C, cstr, ldc, nb, n, q, sign, init); break;
+        default: update_rim_t<3, R>(W, A, astr, C, cstr, ldc, nb, n, q, sign, init); break;
+    }
+}
+
 __device__ __noinline__ void update(double *W, const double *A, size_t astr, const double *C, size_t cstr,
                                     int ldc, int nb, int n, int q, double sign, bool init) {
+    if (q > 8 && q < 32 && (q & 7) == 1) {
+        update_rim<1>(W, A, astr, C, cstr, ldc, nb, n, q, sign, init);
+        return;
+    }
     switch ((q + 7) >> 3) {
         case 1: update_t<1>(W, A, astr, C, cstr, ldc, nb, n, q, sign, init); break;
         case 2: update_t<2>(W, A, astr, C, cstr, ldc, nb, n, q, sign, init); break;

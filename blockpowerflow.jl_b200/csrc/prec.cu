@@ -876,11 +876,11 @@ trsv_sf_kernel(TriKernelArgs t0, TriKernelArgs t1, int p, const double *X, doubl
                 const int col = lane + j * 32;
                 if (col < p) yi[col] = (double)(acc[j] * dv);
             }
+            // publish: the warp barrier orders every lane's row stores before lane 0's release
+            // store, whose gpu-scope release makes them visible to a reader that acquires the
+            // word (happens-before is transitive through the barrier), so no separate fence
             __syncwarp();
-            if (lane == 0) {
-                __threadfence();
-                st_release_u32(flags + i, 2u * epoch + (unsigned)phase);
-            }
+            if (lane == 0) st_release_u32(flags + i, 2u * epoch + (unsigned)phase);
         }
         if (phase == 0) {
             // every CTA reaches this barrier: a warp that gave up still arrives (its CTA's
