@@ -747,7 +747,7 @@ static bpf_status launch_trsv2(bpf_ctx *ctx, const TriDev &t0, const TriDev &t1,
 // taken in level order, position q by warp q mod W (W = all warps of the co-resident grid), and
 // a row waits only for the rows it reads: lane l polls the ready word of the row of entry l
 // (acquire), the warp proceeds when all its lanes have seen theirs.  A producer writes its row,
-// then publishes it (fence + release store of the word).  No deadlock: the pending row of
+// then publishes it (warp barrier + release store of the word).  No deadlock: the pending row of
 // smallest position has all its inputs done (they sit at smaller positions), and its warp is
 // resident (cooperative launch) and has finished its earlier positions, so it runs.  Every poll
 // is bounded by the context's wait limit; a warp that gives up records the timeout and returns,
