@@ -789,68 +789,166 @@ __device__ void spmm_t(const int *__restrict__ rp, const int *__restrict__ ci, c
     }
 }
 
+__device__ __forceinline__ void cpa4(void *smem, const void *gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cpa8(void *smem, const void *gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Per-group staging of the sweeps' coming positions in shared memory (three levels in flight):
+// the row metadata (row, entry range) and the first kG (column, value) pairs and inverted
+// diagonal of each group's first position of a level.
+template <typename TF>
+struct SweepStage {
+    int meta[3][kNG][3];
+    int col[3][kNG][kG];
+    TF val[3][kNG][kG];
+    TF dinv[3][kNG];
+};
+
 // One triangular factor, every level, a __syncthreads between levels.  Y rows of earlier levels
-// are read with plain loads (written by this CTA before the barrier).
+// are read with plain loads (written by this CTA before the barrier).  A group of kG lanes takes
+// positions grp, grp + kNG, ... of each level.  Measured on the batched configuration, a level
+// used to wait for two L2 round trips besides its gathers: the row metadata, then the row's
+// entries (whose addresses need the metadata).  Here they come two and one levels ahead, by
+// asynchronous copies into the shared staging St (a barrier does not wait for them, and they
+// hold no registers): at the start of level l each group issues the entries of its first
+// position of level l + 1 (whose metadata arrived during level l - 1) and the metadata of its
+// first position of level l + 2; every thread waits for its own copies at the end of the level,
+// before the barrier that makes them visible to its group.  A level then waits for the gathers
+// of solved rows (and, in parallel, its rows' right-hand sides) alone.  Positions past the first
+// of a level wider than kNG groups are loaded directly, one ahead.  The summation order is the
+// same as one row at a time.
 template <int CPL, typename TF>
-__device__ void trsv_t(const TriKernelArgs &T, int q, const double *X, double *Y) {
-    const int lane = threadIdx.x & 31, gl = lane & (kG - 1);
+__device__ void trsv_t(const TriKernelArgs &T, int q, const double *X, double *Y, SweepStage<TF> &St) {
+    const int lane = threadIdx.x & 31, gl = lane & (kG - 1), grp = threadIdx.x / kG;
     const unsigned gmask = 0xffu << (lane & ~(kG - 1));
     const TF *val = std::is_same<TF, float>::value ? (const TF *)T.valf : (const TF *)T.val;
     const TF *dinv = std::is_same<TF, float>::value ? (const TF *)T.dinvf : (const TF *)T.dinv;
-    for (int l = 0; l < T.nlev; l++) {
-        const int q1 = __ldg(T.lev_ptr + l + 1);
-        int qq = __ldg(T.lev_ptr + l) + threadIdx.x / kG;
-        int i = 0, rs = 0, re = 0;
-        if (qq < q1) {
-            i = __ldg(T.rows + qq);
-            rs = __ldg(T.rp + qq);
-            re = __ldg(T.rp + qq + 1);
+    const int nl = T.nlev;
+    auto cp_val = [&](TF *dst, const TF *src) {
+        if constexpr (sizeof(TF) == 4) cpa4(dst, src);
+        else cpa8(dst, src);
+    };
+    // metadata of position p into stage s (lane 0 of the group)
+    auto stage_meta = [&](int s, int p) {
+        if (gl == 0) {
+            cpa4(&St.meta[s][grp][0], T.rows + p);
+            cpa4(&St.meta[s][grp][1], T.rp + p);
+            cpa4(&St.meta[s][grp][2], T.rp + p + 1);
         }
-        for (; qq < q1; qq += kNG) {
-            const int qn = qq + kNG;
-            int in = 0, rsn = 0, ren = 0;
-            if (qn < q1) {
-                in = __ldg(T.rows + qn);
-                rsn = __ldg(T.rp + qn);
-                ren = __ldg(T.rp + qn + 1);
-            }
-            TF acc[CPL];
+    };
+    // entries and diagonal of position p into stage s (its metadata already in stage s)
+    auto stage_entries = [&](int s, int p) {
+        const int rs = St.meta[s][grp][1], re = St.meta[s][grp][2];
+        if (rs + gl < re) {
+            cpa4(&St.col[s][grp][gl], T.ci + rs + gl);
+            cp_val(&St.val[s][grp][gl], val + rs + gl);
+        }
+        if (gl == 0 && dinv) cp_val(&St.dinv[s][grp], dinv + p);
+    };
+    // the row at position p with row i, entries [rs, re), first pair (colk, ak), diagonal dv
+    auto solve_row = [&](int i, int rs, int re, int colk, TF ak, TF dv) {
+        TF acc[CPL];
 #pragma unroll
-            for (int c = 0; c < CPL; c++) {
-                const int col = gl + c * kG;
-                acc[c] = col < q ? (TF)X[(size_t)i * q + col] : (TF)0;
-            }
-            for (int kb = rs; kb < re; kb += kG) {
+        for (int c = 0; c < CPL; c++) {
+            const int col = gl + c * kG;
+            acc[c] = col < q ? (TF)X[(size_t)i * q + col] : (TF)0;
+        }
+        for (int kb = rs; kb < re; kb += kG) {
+            if (kb != rs) {
                 const int k = kb + gl;
-                int col = 0;
-                TF a = (TF)0;
+                colk = 0;
+                ak = (TF)0;
                 if (k < re) {
-                    col = __ldg(T.ci + k);
-                    a = val[k];
-                }
-                const int cnt = min(kG, re - kb);
-                #pragma unroll 4   // several entries' loads in flight; same summation order
-                for (int e = 0; e < cnt; e++) {
-                    const int cs = __shfl_sync(gmask, col, e, kG);
-                    const TF as = __shfl_sync(gmask, a, e, kG);
-                    const double *yr = Y + (size_t)cs * q + gl;
-#pragma unroll
-                    for (int c = 0; c < CPL; c++)
-                        if (gl + c * kG < q) acc[c] -= as * (TF)yr[c * kG];
+                    colk = __ldg(T.ci + k);
+                    ak = val[k];
                 }
             }
-            TF dv = (TF)1;
-            if (dinv) dv = dinv[qq];
+            const int cnt = min(kG, re - kb);
+            #pragma unroll 4   // several entries' loads in flight; same summation order
+            for (int e = 0; e < cnt; e++) {
+                const int cs = __shfl_sync(gmask, colk, e, kG);
+                const TF as = __shfl_sync(gmask, ak, e, kG);
+                const double *yr = Y + (size_t)cs * q + gl;
 #pragma unroll
-            for (int c = 0; c < CPL; c++) {
-                const int col = gl + c * kG;
-                if (col < q) Y[(size_t)i * q + col] = (double)(acc[c] * dv);
+                for (int c = 0; c < CPL; c++)
+                    if (gl + c * kG < q) acc[c] -= as * (TF)yr[c * kG];
             }
-            i = in;
-            rs = rsn;
-            re = ren;
         }
-        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < CPL; c++) {
+            const int col = gl + c * kG;
+            if (col < q) Y[(size_t)i * q + col] = (double)(acc[c] * dv);
+        }
+    };
+    // b0 .. b3: starts of levels l .. l + 3 (a level past the last one is empty)
+    int b0 = __ldg(T.lev_ptr), b1 = __ldg(T.lev_ptr + min(1, nl)), b2 = __ldg(T.lev_ptr + min(2, nl)),
+        b3 = __ldg(T.lev_ptr + min(3, nl));
+    // prologue: metadata of levels 0 and 1, then the entries of level 0
+    if (b0 + grp < b1) stage_meta(0, b0 + grp);
+    if (b1 + grp < b2) stage_meta(1, b1 + grp);
+    cpa_commit();
+    cpa_wait_all();
+    __syncthreads();
+    if (b0 + grp < b1) stage_entries(0, b0 + grp);
+    cpa_commit();
+    cpa_wait_all();
+    __syncthreads();
+    for (int l = 0; l < nl; l++) {
+        const int s0 = l % 3, s1 = (l + 1) % 3, s2 = (l + 2) % 3;
+        const int b4 = __ldg(T.lev_ptr + min(l + 4, nl));
+        // asynchronous copies for the coming levels (rows of levels l + 1 and l + 2 are written
+        // only in their own levels)
+        if (b1 + grp < b2) stage_entries(s1, b1 + grp);
+        if (b2 + grp < b3) stage_meta(s2, b2 + grp);
+        cpa_commit();
+        const int p0 = b0 + grp;
+        if (p0 < b1) {
+            const int i = St.meta[s0][grp][0], rs = St.meta[s0][grp][1], re = St.meta[s0][grp][2];
+            const int colk = rs + gl < re ? St.col[s0][grp][gl] : 0;
+            const TF ak = rs + gl < re ? St.val[s0][grp][gl] : (TF)0;
+            const TF dv = dinv ? St.dinv[s0][grp] : (TF)1;
+            solve_row(i, rs, re, colk, ak, dv);
+            // a wide level's further positions, loaded directly one ahead
+            int p = p0 + kNG;
+            int wi = 0, wrs = 0, wre = 0;
+            if (p < b1) {
+                wi = __ldg(T.rows + p);
+                wrs = __ldg(T.rp + p);
+                wre = __ldg(T.rp + p + 1);
+            }
+            for (; p < b1; p += kNG) {
+                const int pw = p + kNG;
+                int ni = 0, nrs = 0, nre = 0;
+                if (pw < b1) {
+                    ni = __ldg(T.rows + pw);
+                    nrs = __ldg(T.rp + pw);
+                    nre = __ldg(T.rp + pw + 1);
+                }
+                int c0 = 0;
+                TF a0 = (TF)0;
+                if (wrs + gl < wre) {
+                    c0 = __ldg(T.ci + wrs + gl);
+                    a0 = val[wrs + gl];
+                }
+                solve_row(wi, wrs, wre, c0, a0, dinv ? dinv[p] : (TF)1);
+                wi = ni;
+                wrs = nrs;
+                wre = nre;
+            }
+        }
+        b0 = b1;
+        b1 = b2;
+        b2 = b3;
+        b3 = b4;
+        cpa_wait_all();   // this thread's copies for levels l + 1 and l + 2 ...
+        __syncthreads();  // ... visible to its group after the barrier
     }
 }
 
@@ -863,20 +961,20 @@ __device__ __noinline__ void spmm(const Sys &S, int q, const double *X, double *
     }
 }
 
-// Z = U^{-1} L^{-1} V
+// Z = U^{-1} L^{-1} V; St: shared staging of the sweeps (in scratch that is dead here)
 template <int CPL, typename TF>
-__device__ __forceinline__ void prec_apply_t(const Sys &S, int q, const double *V, double *Z) {
-    trsv_t<CPL, TF>(S.L, q, V, Z);
-    trsv_t<CPL, TF>(S.U, q, Z, Z);
+__device__ __forceinline__ void prec_apply_t(const Sys &S, int q, const double *V, double *Z, SweepStage<TF> &St) {
+    trsv_t<CPL, TF>(S.L, q, V, Z, St);
+    trsv_t<CPL, TF>(S.U, q, Z, Z, St);
 }
 
 template <typename TF>
-__device__ __noinline__ void prec_apply(const Sys &S, int q, const double *V, double *Z) {
+__device__ __noinline__ void prec_apply(const Sys &S, int q, const double *V, double *Z, SweepStage<TF> &St) {
     switch ((q + kG - 1) / kG) {
-        case 1: prec_apply_t<1, TF>(S, q, V, Z); break;
-        case 2: prec_apply_t<2, TF>(S, q, V, Z); break;
-        case 3: prec_apply_t<3, TF>(S, q, V, Z); break;
-        default: prec_apply_t<4, TF>(S, q, V, Z); break;
+        case 1: prec_apply_t<1, TF>(S, q, V, Z, St); break;
+        case 2: prec_apply_t<2, TF>(S, q, V, Z, St); break;
+        case 3: prec_apply_t<3, TF>(S, q, V, Z, St); break;
+        default: prec_apply_t<4, TF>(S, q, V, Z, St); break;
     }
 }
 
@@ -1319,7 +1417,9 @@ __device__ void solve_unit(const Sys &S, const Unit &U, const IO &io, const Cfg 
         bool brk = false;
         while (j < m && iter < itmax) {
             double *Vj = U.V + j * bs, *Zj = U.Z + j * bs, *Vn = U.V + (j + 1) * bs;
-            prec_apply<TF>(S, q, Vj, Zj);
+            // the Gram / Cholesky / Hessenberg scratch is dead here
+            static_assert(sizeof(SweepStage<double>) <= sizeof(Smem::red), "sweep staging fits the scratch");
+            prec_apply<TF>(S, q, Vj, Zj, *reinterpret_cast<SweepStage<TF> *>(sm.red));
             pc.mark(PH_PREC);
             spmm(S, q, Zj, Vn, nullptr);
             __syncthreads();
