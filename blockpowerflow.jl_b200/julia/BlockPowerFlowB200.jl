@@ -320,16 +320,27 @@ mutable struct BatchPlan
     nrhs::Vector{Int}
 end
 
+# slices: optional widest column slice per system (0: `slice`), as the autotuner's refinement
+# narrows the systems on the critical path (bpf_batch_plan_sliced)
 function BatchPlan(As::Vector{CuSparseMatrixCSR{Float64,Cint}}, nrhs::Vector{Int}; atol=0.0, rtol=1e-8,
-                   itmax=0, memory=0, factor_type=Float32, ordering=:AMD, slice=0, ctas_per_sm=0)
+                   itmax=0, memory=0, factor_type=Float32, ordering=:AMD, slice=0, ctas_per_sm=0,
+                   slices::Union{Nothing,Vector{Int}}=nothing)
     length(As) == length(nrhs) || throw(DimensionMismatch("one nrhs per system expected"))
+    slices === nothing || length(slices) == length(As) ||
+        throw(DimensionMismatch("one slice width per system expected"))
     descs = [desc(A) for A in As]
     opts = Ref(BatchOpts(atol, rtol, itmax, memory, factor_type === Float32 ? 1 : 0,
                          PREC_ORDER[ordering], slice, ctas_per_sm))
     r = Ref{Ptr{Cvoid}}(C_NULL)
-    check(ccall((:bpf_batch_plan, libbpf), Cint,
-                (Ptr{Cvoid}, Cint, Ptr{CsrDesc}, Ptr{Cint}, Ref{BatchOpts}, Ref{Ptr{Cvoid}}),
-                ctx(), length(As), descs, Cint.(nrhs), opts, r))
+    if slices === nothing
+        check(ccall((:bpf_batch_plan, libbpf), Cint,
+                    (Ptr{Cvoid}, Cint, Ptr{CsrDesc}, Ptr{Cint}, Ref{BatchOpts}, Ref{Ptr{Cvoid}}),
+                    ctx(), length(As), descs, Cint.(nrhs), opts, r))
+    else
+        check(ccall((:bpf_batch_plan_sliced, libbpf), Cint,
+                    (Ptr{Cvoid}, Cint, Ptr{CsrDesc}, Ptr{Cint}, Ptr{Cint}, Ref{BatchOpts}, Ref{Ptr{Cvoid}}),
+                    ctx(), length(As), descs, Cint.(nrhs), Cint.(slices), opts, r))
+    end
     P = BatchPlan(r[], As, nrhs)
     finalizer(p -> ccall((:bpf_batch_destroy, libbpf), Cint, (Ptr{Cvoid},), p.h), P)
     return P

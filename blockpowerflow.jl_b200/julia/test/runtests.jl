@@ -148,6 +148,14 @@ end
         @test s.solved
         @test norm(Array(Bk) - M * Array(Xk)) <= 1e-7 * norm(Array(Bk))
     end
+    # a widest slice per system (0 keeps the plan's), in reverse Cuthill-McKee order
+    plan2 = BatchPlan([CuSparseMatrixCSR(M) for M in mats], nrhs; slice=32, ordering=:RCM, slices=[0, 3, 4])
+    st2 = batch_solve!(Xs, plan2, Bs)
+    for (M, Bk, Xk, s) in zip(mats, Bs, Xs, st2)
+        @test s.solved
+        @test norm(Array(Bk) - M * Array(Xk)) <= 1e-7 * norm(Array(Bk))
+    end
+    @test_throws DimensionMismatch BatchPlan([CuSparseMatrixCSR(M) for M in mats], nrhs; slices=[0, 3])
 end
 
 @testset "PowerFlowAssembly (3 buses: slack, PV, PQ)" begin
