@@ -31,10 +31,12 @@
 //    dlarfg convention), one group of lanes per column.
 //  * No cross-CTA waits anywhere: nothing in the batched path can spin.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <numeric>
 #include <type_traits>
+#include <thread>
 #include <vector>
 
 #include "bpf_internal.cuh"
@@ -1751,35 +1753,70 @@ bpf_status bpf_batch_plan_sliced(bpf_ctx *ctx, int nsys, const bpf_csr_desc *A, 
     };
     std::vector<Offs> offs(nsys);
     std::vector<const void *> vals(nsys);
+    // the patterns to the host (one system after another: the context's stream and error state)
+    std::vector<std::vector<int>> arps(nsys), acis(nsys);
     for (int s = 0; s < nsys; s++) {
         const bpf_csr_desc &D = A[s];
         if (D.dtype != BPF_F64) return fail(set_error(ctx, BPF_ERR_NOT_SUPPORTED, "batch: system %d is not FP64", s));
         if (nrhs[s] < 1) return fail(set_error(ctx, BPF_ERR_INVALID_VALUE, "batch: system %d has nrhs < 1", s));
-        std::vector<int> arp, aci, rp, ci, diag, amap, perm;
-        bpf_status st = csr_pattern_to_host(ctx, &D, arp, aci, false, nullptr);
+        bpf_status st = csr_pattern_to_host(ctx, &D, arps[s], acis[s], false, nullptr);
         if (st != BPF_SUCCESS) {
             const std::string msg = ctx->last_error;
             return fail(set_error(ctx, st, "batch: system %d: %s", s, msg.c_str()));
         }
-        const int n = D.n;
-        if (n < 1) return fail(set_error(ctx, BPF_ERR_INVALID_VALUE, "batch: system %d is empty", s));
-        if (o.ordering == BPF_ORDER_NATURAL) {
-            perm.resize(n);
-            std::iota(perm.begin(), perm.end(), 0);
-        } else if (o.ordering == BPF_ORDER_RCM) {
-            perm = order_rcm(n, arp, aci);
-        } else {
-            perm = order_min_degree(n, arp, aci);
-        }
-        const int bad = permute_pattern(n, arp, aci, perm, rp, ci, amap, diag);
-        if (bad >= 0)
-            return fail(set_error(ctx, BPF_ERR_SINGULAR, "batch: system %d: structurally zero diagonal at row %d", s, bad));
-        std::vector<int> pp;
+        if (D.n < 1) return fail(set_error(ctx, BPF_ERR_INVALID_VALUE, "batch: system %d is empty", s));
+    }
+    // the per-system analysis (ordering, permuted pattern, ILU(0) update pairs, level-sorted
+    // factors) is independent host work: host threads take systems from a counter
+    struct SysHost {
+        std::vector<int> rp, ci, diag, amap, perm, pp;
         PairVec pdst, psrc;
-        if (!build_pairs(n, rp.data(), ci.data(), diag.data(), false, pp, pdst, psrc))
+        TriHost L, U;
+        int bad = -1;        // structurally zero diagonal at this row
+        bool pairs_ok = true;
+    };
+    std::vector<SysHost> sh(nsys);
+    {
+        std::atomic<int> next{0};
+        auto work = [&]() {
+            for (int s = next++; s < nsys; s = next++) {
+                SysHost &h = sh[s];
+                const int n = A[s].n;
+                if (o.ordering == BPF_ORDER_NATURAL) {
+                    h.perm.resize(n);
+                    std::iota(h.perm.begin(), h.perm.end(), 0);
+                } else if (o.ordering == BPF_ORDER_RCM) {
+                    h.perm = order_rcm(n, arps[s], acis[s]);
+                } else {
+                    h.perm = order_min_degree(n, arps[s], acis[s]);
+                }
+                h.bad = permute_pattern(n, arps[s], acis[s], h.perm, h.rp, h.ci, h.amap, h.diag);
+                if (h.bad >= 0) continue;
+                h.pairs_ok = build_pairs(n, h.rp.data(), h.ci.data(), h.diag.data(), false, h.pp, h.pdst, h.psrc);
+                if (!h.pairs_ok) continue;
+                h.L = build_tri(n, h.rp.data(), h.ci.data(), h.diag.data(), 0, true);
+                h.U = build_tri(n, h.rp.data(), h.ci.data(), h.diag.data(), 1, false);
+                std::vector<int>().swap(arps[s]);
+                std::vector<int>().swap(acis[s]);
+            }
+        };
+        const int nth = std::max(1, std::min({nsys, 32, (int)std::thread::hardware_concurrency()}));
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nth; t++) pool.emplace_back(work);
+        work();
+        for (auto &th : pool) th.join();
+    }
+    for (int s = 0; s < nsys; s++) {
+        const bpf_csr_desc &D = A[s];
+        SysHost &h = sh[s];
+        if (h.bad >= 0)
+            return fail(set_error(ctx, BPF_ERR_SINGULAR, "batch: system %d: structurally zero diagonal at row %d", s, h.bad));
+        if (!h.pairs_ok)
             return fail(set_error(ctx, BPF_ERR_NOT_SUPPORTED, "batch: system %d: ILU(0) update pairs exceed 2^31 - 1", s));
-        TriHost L = build_tri(n, rp.data(), ci.data(), diag.data(), 0, true);
-        TriHost U = build_tri(n, rp.data(), ci.data(), diag.data(), 1, false);
+        const int n = D.n;
+        std::vector<int> &rp = h.rp, &ci = h.ci, &diag = h.diag, &amap = h.amap, &perm = h.perm, &pp = h.pp;
+        PairVec &pdst = h.pdst, &psrc = h.psrc;
+        TriHost &L = h.L, &U = h.U;
         Offs &f = offs[s];
         f.rp = pk.add(rp);
         f.ci = pk.add(ci);
